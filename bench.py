@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the fine propagator and the one-GPU Parareal driver.
+
+Default workload (one "step"): the fine-propagator throughput configuration --
+256^3 periodic grid, FP64 RK4, c=(1,0.5,0.25), nu=1e-3, dt=5e-5, 500 steps,
+initial field a seeded sum of 8 Fourier modes (wavenumbers 1-4, N(0,1)
+amplitudes).  Metric: cell-updates per second (one cell advanced one RK4
+step), reported in GCUPS, whole job (all ranks), inputs resident in HBM.
+Every field (134 MB) is larger than the 126 MB L2, so no flush is needed
+between timed steps.
+
+`e2e` repeats the same step through the host-buffer C-ABI call
+sp_do_rk4_host: host->device copy of the dense initial field from pinned
+memory, the 500 steps, device->host copy of the result, all inside the timed
+region.
+
+`--impl reference` times the CPU restatement of the reference's OpenMP path
+(oracle/, the reference itself needs Boost and MPI and cannot be built here)
+on the host cores on a bounded sample of the same workload.
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; N>1 under torchrun
+(one independent replica per GPU: the propagator does not shard, "weak"
+scaling with no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Parareal time-to-1e-8 vs serial FP64 fine on 1 B200; fine GCUPS and % HBM roofline"
+UNIT = "GCUPS"
+N_FINE = 256
+STEPS_PER_RUN = 500
+DT = 5e-5
+NU = 1e-3
+C = (1.0, 0.5, 0.25)
+BYTES_PER_CELL_UPDATE = 128  # 16 FP64 field accesses per RK4 step (4 fused stage kernels)
+WORKLOAD = (f"fine RK4 FP64 {N_FINE}^3 x {STEPS_PER_RUN} steps, c=(1,0.5,0.25), nu=1e-3, dt=5e-5, "
+            "8-mode Fourier IC seed 1")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fourier_ic(n, seed=1):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import fourier_modes
+    return fourier_modes(n, seed=seed)
+
+
+def run_reference(args, rank, world):
+    """The CPU restatement of the reference's OpenMP path on the host cores."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    n = N_FINE
+    steps = 2  # bounded sample per step: 2 RK4 steps of the 256^3 workload
+    p = O.params(n, dx=1.0 / n, nu0=NU, nufreq=0.0, cx=C[0], cy=C[1], cz=C[2])
+    q = fourier_ic(n)
+    for _ in range(args.warmup):
+        q1 = O.rk4(p, q, 0.0, DT, steps)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        q1 = O.rk4(p, q, 0.0, DT, steps)
+        times.append(time.perf_counter() - t0)
+    del q1
+    tot = sum(times)
+    val = n ** 3 * steps * args.steps / tot / 1e9
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": f"{steps} RK4 steps of {n}^3 per step"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+                             "sample": f"{steps} RK4 steps of {n}^3 per timed step, {args.steps} steps"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample():
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    n, steps = N_FINE, 24
+    p = O.params(n, dx=1.0 / n, nu0=NU, nufreq=0.0, cx=C[0], cy=C[1], cz=C[2])
+    q = fourier_ic(n)
+    t0 = time.perf_counter()
+    O.rk4(p, q, 0.0, DT, steps)
+    dt = time.perf_counter() - t0
+    return {"value": n ** 3 * steps / dt / 1e9, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+            "sample": f"{steps} RK4 steps of {n}^3 (oracle restating the reference OpenMP path), {dt:.1f} s"}
+
+
+def parareal_summary(torch, sp, device):
+    """Config 3: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import gaussian_noise
+    n, P, T = 128, 32, 0.2
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+    conv.autotune(sp.SP_F64, 1)
+    conv.autotune(sp.SP_F64, P)
+    conv.autotune(sp.SP_F32, 1)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.01, gridSize=n, endTime=T, timeStepsFine=20000,
+                                   timeStepsCoarse=200, kmax=8)
+    q0, qs, q = conv.field(), conv.field(), conv.field()
+    conv.upload(q0, gaussian_noise(n, seed=0))
+    par = sp.Parareal(conv, q0, q, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
+                      tol_kind="reference", skip_converged=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    par.DoSerial()  # warm (graphs)
+    conv.synchronize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    par.DoSerial()
+    conv.synchronize()
+    t_serial = time.perf_counter() - t0
+    ref = par.solution
+    qs.data.copy_(ref.data)
+    par.solution = q
+    rep = par.DoParallel(reference=qs)  # warm (graph capture)
+    rep = par.DoParallel(reference=qs)
+    del ev
+    return {"config": "128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5 (625 steps/slice), coarse RK4 FP32 "
+                      "dt=0.2/224 (200 rounded up to 224 total, 7 steps/slice), Gaussian+noise IC seed 0, "
+                      "c=(1,1,1), nu=0.01",
+            "serial_fine_s": t_serial, "parareal_s": rep["seconds"], "iterations": rep["iterations"],
+            "err_l2_vs_serial": rep["err_l2"][-1] if rep["err_l2"] else None,
+            "defects": rep["defect"], "err_l2": rep["err_l2"],
+            "speedup_vs_serial": t_serial / rep["seconds"] if rep["seconds"] else None,
+            "fine_s": rep["seconds_fine"], "coarse_s": rep["seconds_coarse"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-parareal", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import stencilparareal_b200 as sp
+    from stencilparareal_b200 import build as spbuild
+    spbuild.build()
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local
+    torch.cuda.set_device(device)
+    n = N_FINE
+    conv = sp.Convection(n, n, n, 1.0 / n, NU, 0.0, C[0], C[1], C[2], device=device)
+    tune = conv.autotune(sp.SP_F64, 1)
+    q0 = fourier_ic(n)
+    fin, fout = conv.field(), conv.field()
+    conv.upload(fin, q0)
+    stream = conv.stream
+
+    def one_step():
+        conv.DoRK4(fin, fout, 0.0, DT, STEPS_PER_RUN)
+
+    for _ in range(args.warmup):
+        one_step()
+    conv.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = sp.launch_count()
+    with ClockSampler(device) as clk:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                one_step()
+            e1.record(stream)
+        conv.synchronize()
+        torch.cuda.synchronize()
+    launches = sp.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    t_local = ms / 1e3
+    if dist:
+        t = torch.tensor([t_local], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        dist.barrier()
+    else:
+        t_max = t_local
+    cells = n ** 3 * STEPS_PER_RUN * args.steps
+    value = cells * world / t_max / 1e9
+
+    # e2e: host buffers through the C ABI (pinned), copies inside the timed region
+    h_in = torch.from_numpy(q0).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    lib = sp._lib.lib()
+    conv.call(lib.sp_do_rk4_host, conv.handle, h_in.data_ptr(), h_out.data_ptr(), 0.0, DT, STEPS_PER_RUN)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        conv.call(lib.sp_do_rk4_host, conv.handle, h_in.data_ptr(), h_out.data_ptr(), 0.0, DT, STEPS_PER_RUN)
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = cells * world / t_e2e / 1e9
+
+    peak, peak_kind = peaks()
+    achieved = BYTES_PER_CELL_UPDATE * n ** 3 * STEPS_PER_RUN * args.steps / t_local / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f).get("stage_kernel_bytes_per_cell_update")
+        except Exception:
+            traffic = None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (each 256^3 FP64 field is 134 MB)",
+                       "parallelism": f"replicas x{world}", "tune": tune},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
+                    "d2h_bytes_per_step": int(h_out.numel() * 8)},
+            "gpu_launches": int(launches), "clocks": clk.summary()}
+    if rank == 0 and world == 1:
+        if not args.no_parareal:
+            try:
+                line["parareal"] = parareal_summary(torch, sp, device)
+            except Exception as ex:  # reported, not hidden
+                line["parareal"] = {"error": repr(ex)}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

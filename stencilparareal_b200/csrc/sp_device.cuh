@@ -1,0 +1,133 @@
+// sp_device.cuh -- device-side building blocks: PTX wrappers for mbarriers and
+// TMA tensor loads (sm_90+/sm_100a), 16-byte vector access, bounded waits.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace sp {
+
+// A bounded wait gives up after this many nanoseconds of %globaltimer, sets
+// the device error word and lets the kernel return (no trap, no endless spin).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+// Device error word values.
+enum : int { DEV_OK = 0, DEV_WAIT_TIMEOUT = 1 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses to the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of the barrier; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
+// 3-D tiled TMA load global -> shared, completion signalled on `bar`
+// (transaction bytes).  No multicast: the tensor always lies in this GPU's HBM.
+__device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* tm, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* tm) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
+}
+
+// ---- 16-byte vectors --------------------------------------------------------
+template <typename T>
+struct V16;
+template <>
+struct V16<double> {
+    static constexpr int N = 2;
+};
+template <>
+struct V16<float> {
+    static constexpr int N = 4;
+};
+
+template <typename T, int N>
+struct Vec {
+    T v[N];
+};
+
+template <typename T>
+__device__ __forceinline__ Vec<T, V16<T>::N> ld16(const T* p) {
+    Vec<T, V16<T>::N> r;
+    if constexpr (sizeof(T) == 8) {
+        const double2 d = *reinterpret_cast<const double2*>(p);
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else {
+        const float4 d = *reinterpret_cast<const float4*>(p);
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+        r.v[2] = d.z;
+        r.v[3] = d.w;
+    }
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void st16(T* p, const Vec<T, V16<T>::N>& r) {
+    if constexpr (sizeof(T) == 8) {
+        *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+    } else {
+        *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T fmaT(T a, T b, T c) {
+    if constexpr (sizeof(T) == 8) return fma(a, b, c);
+    else return fmaf(a, b, c);
+}
+
+}  // namespace sp

@@ -1,0 +1,104 @@
+// sp_internal.h -- shared host-side declarations of the B200 propagator library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace sp {
+
+// Geometry of one field in HBM (see sp_field_layout in include/sp_abi.h).
+struct Geo {
+    int ni = 0, nj = 0, nk = 0;
+    int lx = 0;         // columns left of interior i = 0 (16 bytes worth)
+    int es = 0;         // element size in bytes
+    long long px = 0, py = 0, pz = 0, plane = 0, origin = 0, total = 0;
+};
+
+Geo make_geo(int ni, int nj, int nk, int es);
+
+// Kernel families.
+enum Op : int {
+    OP_RK_S1 = 0,  // k=R(q);  y=q+(dt/2)k;  a=q+(dt/6)k
+    OP_RK_S2 = 1,  // k=R(y);  y'=q+(dt/2)k; a+=(dt/3)k
+    OP_RK_S3 = 2,  // k=R(y);  y'=q+dt k;    a+=(dt/3)k
+    OP_RK_S4 = 3,  // k=R(y);  out=a+(dt/6)k
+    OP_EULER = 4,  // k=R2(y); out=y+dt k
+    OP_ADJ = 5,    // adjoint stage (see sp_adjoint.cu)
+    OP_COUNT = 6
+};
+
+// Launch-shape choice for the stage kernels.
+struct Tune {
+    int ty = 8;       // rows of a CTA tile (warps per CTA for the TMA kernel)
+    int zchunk = 32;  // planes marched by one CTA
+    int tma = 1;      // 1: TMA/mbarrier pipeline kernel; 0: direct-load kernel
+};
+
+// Coefficients of the right-hand side, precomputed on the host.
+struct Coef {
+    // RHS4: R = cax*(8(q-1 - q+1) - (q-2 - q+2))_x + ... + nu*s4*(16 S1 - S2 - 90 q)
+    double ca[3] = {0, 0, 0};  // c_d / (12 dx)
+    double s4 = 0;             // 1 / (12 dx^2)
+    // RHS2: R2 = sum_d u_d * dq_d + nu*s2*(S1 - 6q), dq_d per mode
+    double u[3] = {0, 0, 0};
+    int mode[3] = {0, 0, 0};   // 0: q - q[-1] (upwind, c>0); 1: q[+1] - q (upwind, c<=0); 2: q[-1] - q[+1] (central)
+    double s2 = 0;             // 1 / dx^2
+    double dx = 0;
+};
+
+Coef make_coef(double dx, double cx, double cy, double cz, int upwind);
+
+// One stage launch over `items` fields stored back to back (item stride = geo.total).
+struct StageLaunch {
+    int op = OP_RK_S1;
+    int prec = 0;                    // 0: FP64, 1: FP32
+    const void* yin = nullptr;       // stencil input (field base of item 0)
+    const void* q = nullptr;         // step-start field (S2, S3)
+    void* acc = nullptr;             // accumulator (S1 writes, S2/S3 read+write, S4 reads)
+    void* yout = nullptr;            // stencil output (written with periodic images)
+    int items = 1;
+    const int* item_lo = nullptr;    // device word: items below it are skipped (may be null)
+    int item_base = 0;               // index of item 0 in the item_lo numbering
+    double nu = 0;                   // diffusivity (all items) ...
+    const double* nu_items = nullptr;// ... or one value per item (device)
+    double c_y = 0, c_acc = 0;       // stage coefficients
+    Coef coef;
+    // adjoint extras
+    const void* ypt = nullptr;       // forward stage value (pointwise)
+    const void* lam = nullptr;       // adjoint of the step end (pointwise)
+    void* lam_acc = nullptr;         // accumulated adjoint of the step start
+    double* par_acc = nullptr;       // 4 partial sums (nu, cx, cy, cz) for the parameter gradient
+    double c_lam = 0, c_ybar = 0;    // mu_{s-1} = c_lam*lam + c_ybar*ybar_s
+    double sigma = 1;                // mu_s = sigma * (stencil input)
+    double dnu = 1;                  // d nu / d nu0
+    int adj_first = 0;               // 1: lam_acc = lam + ybar (first adjoint stage of a step)
+};
+
+// Launches one stage kernel; counts the launch.  err: device error word.
+cudaError_t launch_stage(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err);
+
+// Pointwise helpers.
+cudaError_t launch_periodicity(const Geo& g, void* field, int items, cudaStream_t s);
+cudaError_t launch_dense_to_field(const Geo& g, const void* dense, int dense_prec, void* field, cudaStream_t s);
+cudaError_t launch_field_to_dense(const Geo& g, const void* field, void* dense, int dense_prec, cudaStream_t s);
+// dst (geo gd, precision of gd.es) <- src (geo gs), interior with images.
+cudaError_t launch_convert(const Geo& gd, void* dst, const Geo& gs, const void* src, cudaStream_t s,
+                           const int* item_lo = nullptr, int item = 0);
+// Sets the dynamic shared-memory limit of every TMA stage kernel on the current device.
+cudaError_t prepare_kernels();
+// Parareal correction: Q = (gnew + f) - gold written to u_next (FP64, with images);
+// gold <- gnew; defect sums (sum (Q-u_old)^2, sum Q^2) atomically added to def[0..1].
+cudaError_t launch_update(const Geo& g64, const Geo& gc, const void* gnew, const double* f, void* gold,
+                          double* u_next, double* def, const int* item_lo, int item, cudaStream_t s);
+// err[0] += sum (a-b)^2 ; err[1] += sum b^2 ; err[2] = max |a-b| ; err[3] = max |a|   (FP64 fields)
+cudaError_t launch_errors(const Geo& g, const double* a, const double* b, double* acc4, cudaStream_t s);
+// Pointwise axpby on FP64 fields (interior+images): out = alpha*x + beta*y (y may be null).
+cudaError_t launch_axpby(const Geo& g, double* out, double alpha, const double* x, double beta, const double* y,
+                         cudaStream_t s);
+// 0.5*||a-b||^2 and lam = a - b (lam may alias nothing; written with images).
+cudaError_t launch_misfit(const Geo& g, const double* a, const double* b, double* lam, double* jacc, cudaStream_t s);
+
+long long launches();
+void add_launches(long long n);
+
+}  // namespace sp

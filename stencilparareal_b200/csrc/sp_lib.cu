@@ -1,0 +1,991 @@
+// sp_lib.cu -- the C ABI (include/sp_abi.h): propagator handles, the time-step
+// loop (CUDA-graph chunks), the one-GPU Parareal driver, the adjoint.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/sp_abi.h"
+#include "sp_internal.h"
+
+using namespace sp;
+
+// ---------------------------------------------------------------------------
+// Errors.
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define SP_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(SP_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                         \
+    } while (0)
+
+// computenu (Convection.h:81-84)
+inline double computenu(double nu0, double nufreq, double t) { return nu0 * (1. + .5 * std::sin(nufreq * t)); }
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) { p = nullptr; return e; }
+        bytes = n;
+        return cudaMemset(p, 0, n);
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Propagator handle.
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;
+};
+
+struct sp_convection {
+    sp_params P{};
+    int device = 0;
+    Geo g[2];          // [0] FP64, [1] FP32
+    Coef coef;
+    cudaStream_t own = nullptr, user = nullptr;
+    DevBuf scratch[2];  // per precision: ya, yb, acc (x batch) for DoRK4 / Euler ping-pong
+    int scratch_items[2] = {0, 0};
+    DevBuf err;         // device error word
+    DevBuf red;         // reduction scratch (8 doubles)
+    DevBuf dense;       // staging for the host-buffer entry point
+    std::map<std::tuple<int, int>, Tune> tunes;  // (prec, items) -> tune
+    std::map<std::tuple<int, const void*, double, double, int>, GraphEntry> graphs;
+    cudaStream_t stream() const { return user ? user : own; }
+    ~sp_convection() {
+        for (auto& kv : graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (own) cudaStreamDestroy(own);
+    }
+    Tune tune(int prec, int items) {
+        auto it = tunes.find({prec, items});
+        if (it != tunes.end()) return it->second;
+        Tune t;
+        // default before tuning: TMA pipeline, 8-row tiles, z-chunks that give
+        // at least ~4 CTAs per SM
+        const int VX = prec == 0 ? 2 : 4;
+        const long long tiles = (long long)((P.ni + 32 * VX - 1) / (32 * VX)) * ((P.nj + 7) / 8) * items;
+        int zc = P.nk;
+        while (zc > 8 && tiles * ((P.nk + zc - 1) / zc) < 148LL * 4) zc = (zc + 1) / 2;
+        t.zchunk = std::max(1, zc);
+        return t;
+    }
+    void drop_graphs() {
+        for (auto& kv : graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
+    }
+    int ensure_scratch(int prec, int items) {
+        if (scratch_items[prec] >= items) return SP_OK;
+        drop_graphs();  // captured graphs hold the old scratch addresses
+        const size_t n = (size_t)3 * items * g[prec].total * g[prec].es;
+        cudaError_t e = scratch[prec].alloc(n);
+        if (e != cudaSuccess) return fail(SP_ERR_NOMEM, "scratch allocation of %zu bytes: %s", n, cudaGetErrorString(e));
+        scratch_items[prec] = items;
+        return SP_OK;
+    }
+    void* sbuf(int prec, int which, int items) const {
+        return static_cast<char*>(scratch[prec].p) + (size_t)which * items * g[prec].total * g[prec].es;
+    }
+};
+
+namespace {
+
+int check_handle(sp_convection* h) {
+    if (!h) return fail(SP_ERR_INVALID, "null handle");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "cudaSetDevice(%d): %s", h->device, cudaGetErrorString(e));
+    return SP_OK;
+}
+
+// Per-item diffusivity source for a stage launch.
+struct NuSrc {
+    double nu = 0;
+    const double* items = nullptr;
+};
+
+// One RK4 step over `items` fields: in -> out, with scratch ya/yb/acc.
+cudaError_t enqueue_rk4_step3(const Geo& g, int prec, const Coef& c, double dt, NuSrc nu, const void* in, void* out,
+                              void* ya, void* yb, void* yc, void* acc, int items, const int* item_lo, int item_base,
+                              const Tune& t, cudaStream_t s, int* err) {
+    StageLaunch L;
+    L.prec = prec;
+    L.items = items;
+    L.item_lo = item_lo;
+    L.item_base = item_base;
+    L.nu = nu.nu;
+    L.nu_items = nu.items;
+    L.coef = c;
+    const double dthalf = dt * .5;  // Convection.cpp:320
+    // S1
+    L.op = OP_RK_S1; L.yin = in; L.yout = ya; L.acc = acc; L.c_y = dthalf; L.c_acc = dt / 6.;
+    cudaError_t e = launch_stage(g, L, t, s, err);
+    if (e != cudaSuccess) return e;
+    // S2
+    L.op = OP_RK_S2; L.yin = ya; L.q = in; L.yout = yb; L.c_y = dthalf; L.c_acc = dt / 3.;
+    if ((e = launch_stage(g, L, t, s, err)) != cudaSuccess) return e;
+    // S3
+    L.op = OP_RK_S3; L.yin = yb; L.q = in; L.yout = yc; L.c_y = dt; L.c_acc = dt / 3.;
+    if ((e = launch_stage(g, L, t, s, err)) != cudaSuccess) return e;
+    // S4
+    L.op = OP_RK_S4; L.yin = yc; L.q = nullptr; L.yout = out; L.c_acc = dt / 6.;
+    return launch_stage(g, L, t, s, err);
+}
+
+cudaError_t enqueue_rk4_step(const Geo& g, int prec, const Coef& c, double dt, NuSrc nu, const void* in, void* out,
+                             void* ya, void* yb, void* acc, int items, const int* item_lo, int item_base,
+                             const Tune& t, cudaStream_t s, int* err) {
+    return enqueue_rk4_step3(g, prec, c, dt, nu, in, out, ya, yb, ya, acc, items, item_lo, item_base, t, s, err);
+}
+
+cudaError_t enqueue_euler_step(const Geo& g, int prec, const Coef& c, double dt, NuSrc nu, const void* in, void* out,
+                               int items, const int* item_lo, int item_base, const Tune& t, cudaStream_t s,
+                               int* err) {
+    StageLaunch L;
+    L.op = OP_EULER;
+    L.prec = prec;
+    L.items = items;
+    L.item_lo = item_lo;
+    L.item_base = item_base;
+    L.nu = nu.nu;
+    L.nu_items = nu.items;
+    L.coef = c;
+    L.yin = in;
+    L.yout = out;
+    L.c_y = dt;
+    return launch_stage(g, L, t, s, err);
+}
+
+// Graph of `n` in-place RK4 steps on a single field (constant nu).
+int get_chunk_graph(sp_convection* h, int prec, void* field, double dt, double nu, int n, GraphEntry** out) {
+    auto key = std::make_tuple(prec, (const void*)field, dt, nu, n);
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) { *out = &it->second; return SP_OK; }
+    if (h->graphs.size() > 32) {  // bounded cache
+        for (auto& kv : h->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        h->graphs.clear();
+    }
+    int rc = h->ensure_scratch(prec, 1);
+    if (rc) return rc;
+    const Tune t = h->tune(prec, 1);
+    cudaStream_t s = h->stream();
+    SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    const long long before = launches();
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+        e = enqueue_rk4_step(h->g[prec], prec, h->coef, dt, NuSrc{nu, nullptr}, field, field, h->sbuf(prec, 0, 1),
+                             h->sbuf(prec, 1, 1), h->sbuf(prec, 2, 1), 1, nullptr, 0, t, s, h->err.as<int>());
+    const long long nodes = launches() - before;
+    add_launches(-nodes);  // captured, not launched
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return fail(SP_ERR_CUDA, "capture: %s", cudaGetErrorString(e)); }
+    if (e2 != cudaSuccess) return fail(SP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+    GraphEntry ge;
+    e = cudaGraphInstantiate(&ge.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    ge.nodes = nodes;
+    auto res = h->graphs.emplace(key, ge);
+    *out = &res.first->second;
+    return SP_OK;
+}
+
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &st);
+    return st != cudaStreamCaptureStatusNone;
+}
+
+constexpr int kChunk = 50;  // RK4 steps per captured graph
+
+// Convection::DoRK4 / DoEuler on single fields of precision prec.
+int do_prop(sp_convection* h, int prec, bool rk, const void* in, void* out, double tStart, double dt, int n) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!in || !out) return fail(SP_ERR_INVALID, "null field");
+    if (n < 0) return fail(SP_ERR_INVALID, "negative step count");
+    if (n == 0) return SP_OK;  // Convection.cpp:296: no step, output untouched
+    if ((rc = h->ensure_scratch(prec, 1))) return rc;
+    const Geo& g = h->g[prec];
+    cudaStream_t s = h->stream();
+    int* err = h->err.as<int>();
+    const Tune t = h->tune(prec, 1);
+    // Periodicity on the input, in place, as before the reference's first stencil.
+    SP_CUDA(launch_periodicity(g, const_cast<void*>(in), 1, s));
+    const bool const_nu = h->P.nufreq == 0.;
+    if (rk) {
+        SP_CUDA(enqueue_rk4_step(g, prec, h->coef, dt, NuSrc{computenu(h->P.nu0, h->P.nufreq, tStart), nullptr}, in,
+                                 out, h->sbuf(prec, 0, 1), h->sbuf(prec, 1, 1), h->sbuf(prec, 2, 1), 1, nullptr, 0, t,
+                                 s, err));
+        int i = 0;
+        int left = n - 1;
+        if (const_nu && !capturing(s)) {
+            const double nu = computenu(h->P.nu0, h->P.nufreq, tStart);
+            if (left >= kChunk) {
+                GraphEntry* ge = nullptr;
+                if ((rc = get_chunk_graph(h, prec, out, dt, nu, kChunk, &ge))) return rc;
+                while (left >= kChunk) {
+                    SP_CUDA(cudaGraphLaunch(ge->exec, s));
+                    add_launches(ge->nodes);
+                    left -= kChunk;
+                    i += kChunk;
+                }
+            }
+        }
+        for (; left > 0; --left) {
+            const double tt = tStart + (++i) * dt;  // Convection.cpp:302
+            SP_CUDA(enqueue_rk4_step(g, prec, h->coef, dt, NuSrc{computenu(h->P.nu0, h->P.nufreq, tt), nullptr}, out,
+                                     out, h->sbuf(prec, 0, 1), h->sbuf(prec, 1, 1), h->sbuf(prec, 2, 1), 1, nullptr, 0,
+                                     t, s, err));
+        }
+    } else {
+        // Euler: one fused pass per step (out = in + dt R2(in)) needs distinct
+        // input and output, so steps alternate between `out` and scratch.
+        void* tmp = h->sbuf(prec, 0, 1);
+        const void* src = in;
+        for (int i = 0; i < n; ++i) {
+            const double tt = i == 0 ? tStart : tStart + i * dt;
+            // pick the destination so that the last step lands in `out`
+            void* dst = ((n - 1 - i) % 2 == 0) ? out : tmp;
+            if (dst == src) dst = (dst == out) ? tmp : out;
+            SP_CUDA(enqueue_euler_step(g, prec, h->coef, dt, NuSrc{computenu(h->P.nu0, h->P.nufreq, tt), nullptr}, src,
+                                       dst, 1, nullptr, 0, t, s, err));
+            src = dst;
+        }
+        if (src != out) {
+            SP_CUDA(cudaMemcpyAsync(out, src, g.total * g.es, cudaMemcpyDeviceToDevice, s));
+        }
+    }
+    return SP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI.
+extern "C" {
+
+const char* sp_last_error(void) { return g_err.c_str(); }
+int sp_abi_version(void) { return SP_ABI_VERSION; }
+long long sp_launch_count(void) { return launches(); }
+
+int sp_field_layout(int ni, int nj, int nk, int precision, sp_layout* out) {
+    if (!out || ni < 2 || nj < 2 || nk < 2 || (precision != SP_F64 && precision != SP_F32))
+        return fail(SP_ERR_INVALID, "sp_field_layout: grid must be at least 2^3 and precision SP_F64/SP_F32");
+    const Geo g = make_geo(ni, nj, nk, precision == SP_F64 ? 8 : 4);
+    out->ni = ni; out->nj = nj; out->nk = nk; out->lx = g.lx; out->elem_size = g.es;
+    out->px = g.px; out->py = g.py; out->pz = g.pz; out->plane = g.plane; out->origin = g.origin;
+    out->total = g.total;
+    return SP_OK;
+}
+
+int sp_convection_create(const sp_params* p, int device, sp_convection** out) {
+    if (!p || !out) return fail(SP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (p->ni < 2 || p->nj < 2 || p->nk < 2) return fail(SP_ERR_INVALID, "grid %dx%dx%d: every axis needs >= 2 cells", p->ni, p->nj, p->nk);
+    if (!(p->dx > 0)) return fail(SP_ERR_INVALID, "dx must be positive");
+    if ((long long)p->nk + 4 > 65535LL * 8) return fail(SP_ERR_INVALID, "nk too large");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SP_ERR_UNSUPPORTED, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(SP_ERR_INVALID, "device %d out of range", device);
+    SP_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    SP_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(SP_ERR_UNSUPPORTED, "this library is built for sm_100a (found sm_%d%d)", prop.major, prop.minor);
+    std::unique_ptr<sp_convection> h(new sp_convection());
+    h->P = *p;
+    h->device = device;
+    h->g[0] = make_geo(p->ni, p->nj, p->nk, 8);
+    h->g[1] = make_geo(p->ni, p->nj, p->nk, 4);
+    h->coef = make_coef(p->dx, p->cx, p->cy, p->cz, p->upwind);
+    SP_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+    if (h->err.alloc(64) != cudaSuccess) return fail(SP_ERR_NOMEM, "error word");
+    if (h->red.alloc(64 * sizeof(double)) != cudaSuccess) return fail(SP_ERR_NOMEM, "reduction scratch");
+    SP_CUDA(prepare_kernels());
+    *out = h.release();
+    return SP_OK;
+}
+
+int sp_convection_destroy(sp_convection* h) {
+    if (!h) return SP_OK;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream());
+    delete h;
+    return SP_OK;
+}
+
+int sp_convection_set_stream(sp_convection* h, void* stream) {
+    if (!h) return fail(SP_ERR_INVALID, "null handle");
+    h->user = static_cast<cudaStream_t>(stream);
+    return SP_OK;
+}
+
+int sp_convection_synchronize(sp_convection* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    SP_CUDA(cudaStreamSynchronize(h->stream()));
+    int word = 0;
+    SP_CUDA(cudaMemcpy(&word, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (word != 0) {
+        cudaMemset(h->err.p, 0, sizeof(int));
+        return fail(SP_ERR_TIMEOUT, "a bounded in-kernel wait gave up (device error word %d)", word);
+    }
+    return SP_OK;
+}
+
+int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int tma) {
+    if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
+    if (ty != 4 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "ty must be 4, 8 or 16");
+    if (zchunk < 1) return fail(SP_ERR_INVALID, "zchunk must be >= 1");
+    Tune t;
+    t.ty = ty;
+    t.zchunk = zchunk;
+    t.tma = tma ? 1 : 0;
+    h->tunes[{precision, batch}] = t;
+    for (auto& kv : h->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    h->graphs.clear();
+    return SP_OK;
+}
+
+int sp_tuned_config(sp_convection* h, int precision, int batch, int* ty, int* zchunk, int* tma) {
+    if (!h) return fail(SP_ERR_INVALID, "null handle");
+    const Tune t = h->tune(precision, batch);
+    if (ty) *ty = t.ty;
+    if (zchunk) *zchunk = t.zchunk;
+    if (tma) *tma = t.tma;
+    return SP_OK;
+}
+
+int sp_do_rk4(sp_convection* h, const double* in, double* out, double tStart, double dt, int timesteps) {
+    return do_prop(h, 0, true, in, out, tStart, dt, timesteps);
+}
+int sp_do_euler(sp_convection* h, const double* in, double* out, double tStart, double dt, int timesteps) {
+    return do_prop(h, 0, false, in, out, tStart, dt, timesteps);
+}
+int sp_do_rk4_timestep(sp_convection* h, const double* in, double* out, double t, double dt) {
+    return do_prop(h, 0, true, in, out, t, dt, 1);
+}
+int sp_do_euler_timestep(sp_convection* h, const double* in, double* out, double t, double dt) {
+    return do_prop(h, 0, false, in, out, t, dt, 1);
+}
+int sp_do_rk4_f32(sp_convection* h, const float* in, float* out, double tStart, double dt, int timesteps) {
+    return do_prop(h, 1, true, in, out, tStart, dt, timesteps);
+}
+int sp_do_euler_f32(sp_convection* h, const float* in, float* out, double tStart, double dt, int timesteps) {
+    return do_prop(h, 1, false, in, out, tStart, dt, timesteps);
+}
+
+int sp_periodicity_apply(sp_convection* h, void* field, int precision) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!field || (precision != SP_F64 && precision != SP_F32)) return fail(SP_ERR_INVALID, "bad field/precision");
+    SP_CUDA(launch_periodicity(h->g[precision], field, 1, h->stream()));
+    return SP_OK;
+}
+
+int sp_field_import(sp_convection* h, const void* dense, void* field, int precision, int dense_on_host) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dense || !field || (precision != SP_F64 && precision != SP_F32)) return fail(SP_ERR_INVALID, "bad args");
+    const Geo& g = h->g[precision];
+    cudaStream_t s = h->stream();
+    const void* src = dense;
+    if (dense_on_host) {
+        const size_t n = (size_t)g.ni * g.nj * g.nk * g.es;
+        if (h->dense.alloc(n) != cudaSuccess) return fail(SP_ERR_NOMEM, "staging");
+        SP_CUDA(cudaMemcpyAsync(h->dense.p, dense, n, cudaMemcpyHostToDevice, s));
+        src = h->dense.p;
+    }
+    SP_CUDA(launch_dense_to_field(g, src, precision, field, s));
+    return SP_OK;
+}
+
+int sp_field_export(sp_convection* h, const void* field, void* dense, int precision, int dense_on_host) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dense || !field || (precision != SP_F64 && precision != SP_F32)) return fail(SP_ERR_INVALID, "bad args");
+    const Geo& g = h->g[precision];
+    cudaStream_t s = h->stream();
+    if (dense_on_host) {
+        const size_t n = (size_t)g.ni * g.nj * g.nk * g.es;
+        if (h->dense.alloc(n) != cudaSuccess) return fail(SP_ERR_NOMEM, "staging");
+        SP_CUDA(launch_field_to_dense(g, field, h->dense.p, precision, s));
+        SP_CUDA(cudaMemcpyAsync(dense, h->dense.p, n, cudaMemcpyDeviceToHost, s));
+        SP_CUDA(cudaStreamSynchronize(s));
+    } else {
+        SP_CUDA(launch_field_to_dense(g, field, dense, precision, s));
+    }
+    return SP_OK;
+}
+
+int sp_do_rk4_host(sp_convection* h, const double* in_host, double* out_host, double tStart, double dt,
+                   int timesteps) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!in_host || !out_host) return fail(SP_ERR_INVALID, "null host buffer");
+    if (timesteps < 0) return fail(SP_ERR_INVALID, "negative step count");
+    if ((rc = h->ensure_scratch(0, 2))) return rc;  // fields 3 and 4 of the 2-item scratch hold in/out
+    const Geo& g = h->g[0];
+    double* f_in = static_cast<double*>(h->sbuf(0, 3, 1));
+    double* f_out = static_cast<double*>(h->sbuf(0, 4, 1));
+    if ((rc = sp_field_import(h, in_host, f_in, SP_F64, 1))) return rc;
+    if (timesteps == 0) {
+        SP_CUDA(cudaMemcpyAsync(f_out, f_in, g.total * g.es, cudaMemcpyDeviceToDevice, h->stream()));
+    } else if ((rc = sp_do_rk4(h, f_in, f_out, tStart, dt, timesteps))) {
+        return rc;
+    }
+    if ((rc = sp_field_export(h, f_out, out_host, SP_F64, 1))) return rc;
+    return sp_convection_synchronize(h);
+}
+
+int sp_field_errors(sp_convection* h, const double* a, const double* b, double* err_max, double* err_l2) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!a || !b) return fail(SP_ERR_INVALID, "null field");
+    cudaStream_t s = h->stream();
+    SP_CUDA(cudaMemsetAsync(h->red.p, 0, 4 * sizeof(double), s));
+    SP_CUDA(launch_errors(h->g[0], a, b, h->red.as<double>(), s));
+    double r[4];
+    SP_CUDA(cudaMemcpyAsync(r, h->red.p, sizeof r, cudaMemcpyDeviceToHost, s));
+    SP_CUDA(cudaStreamSynchronize(s));
+    if (err_max) *err_max = r[2] / r[3];
+    if (err_l2) *err_l2 = std::sqrt(r[0] / r[1]);
+    return SP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: times the S2 stage (the most common kernel: one stencil input,
+// two pointwise inputs, two outputs) for each candidate launch shape.
+extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if ((precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad args");
+    cudaStream_t s = h->stream();
+    if (capturing(s)) return fail(SP_ERR_STATE, "cannot tune while the stream is capturing");
+    const Geo& g = h->g[precision];
+    DevBuf buf;
+    const size_t fb = (size_t)batch * g.total * g.es;
+    if (buf.alloc(5 * fb) != cudaSuccess) return fail(SP_ERR_NOMEM, "tuning buffers");
+    char* p = buf.as<char>();
+    cudaEvent_t e0, e1;
+    SP_CUDA(cudaEventCreate(&e0));
+    SP_CUDA(cudaEventCreate(&e1));
+    StageLaunch L;
+    L.op = OP_RK_S2;
+    L.prec = precision;
+    L.items = batch;
+    L.coef = h->coef;
+    L.nu = h->P.nu0;
+    L.yin = p; L.q = p + fb; L.acc = p + 2 * fb; L.yout = p + 3 * fb;
+    L.c_y = 1e-9; L.c_acc = 1e-9;
+    Tune best;
+    float best_ms = 1e30f;
+    std::vector<int> zcs = {4, 8, 16, 32, 64};
+    zcs.push_back(g.nk);
+    for (int tma = 1; tma >= 0; --tma)
+        for (int ty : {4, 8, 16})
+            for (int zc : zcs) {
+                if (zc > g.nk && zc != g.nk) continue;
+                Tune t;
+                t.tma = tma; t.ty = ty; t.zchunk = zc;
+                if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
+                cudaError_t e = launch_stage(g, L, t, s, h->err.as<int>());
+                if (e != cudaSuccess) { cudaGetLastError(); continue; }
+                float ms = 1e30f;
+                for (int r = 0; r < 3; ++r) {
+                    cudaEventRecord(e0, s);
+                    launch_stage(g, L, t, s, h->err.as<int>());
+                    cudaEventRecord(e1, s);
+                    cudaEventSynchronize(e1);
+                    float m = 0;
+                    cudaEventElapsedTime(&m, e0, e1);
+                    ms = std::min(ms, m);
+                }
+                if (ms < best_ms) { best_ms = ms; best = t; }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    SP_CUDA(cudaStreamSynchronize(s));
+    h->tunes[{precision, batch}] = best;
+    for (auto& kv : h->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    h->graphs.clear();
+    return SP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Parareal.
+struct sp_parareal {
+    sp_convection* prop = nullptr;
+    sp_parareal_cfg cfg{};
+    int P = 0, tsF = 0, tsC = 0;
+    double dtF = 0, dtC = 0, slice = 0;
+    int cprec = 0;         // coarse precision index
+    Geo g64, gc;
+    DevBuf U;              // P+1 FP64 fields: slice inputs U_0..U_{P-1}, last slice result U_P
+    DevBuf F;              // P FP64 fields: fine results
+    DevBuf fs;             // 3P FP64 fields: fine scratch ya, yb, acc
+    DevBuf Gold;           // P coarse fields
+    DevBuf Gt;             // 2 coarse fields (coarse result / ping-pong) + 3 coarse scratch
+    DevBuf ctl;            // device control: item_lo (int) + defect sums (2P doubles) + err4
+    DevBuf nutab;          // fine nu table (tsF x P) when nufreq != 0
+    int* h_itemlo = nullptr;   // pinned
+    double* h_def = nullptr;   // pinned, 2P + 4
+    cudaGraphExec_t iter = nullptr;
+    long long iter_nodes = 0;
+    int coarse_res = 0;    // which Gt buffer holds the coarse result after a sweep step
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    ~sp_parareal() {
+        if (iter) cudaGraphExecDestroy(iter);
+        if (h_itemlo) cudaFreeHost(h_itemlo);
+        if (h_def) cudaFreeHost(h_def);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    double* u(int r) const { return U.as<double>() + (size_t)r * g64.total; }
+    double* f(int r) const { return F.as<double>() + (size_t)r * g64.total; }
+    void* gold(int r) const { return static_cast<char*>(Gold.p) + (size_t)r * gc.total * gc.es; }
+    void* gt(int i) const { return static_cast<char*>(Gt.p) + (size_t)i * gc.total * gc.es; }
+    int* itemlo() const { return static_cast<int*>(ctl.p); }
+    double* def() const { return reinterpret_cast<double*>(static_cast<char*>(ctl.p) + 256); }
+    double* err4() const { return def() + 2 * P; }
+};
+
+namespace {
+
+// Coarse propagation G of one field: src (FP64 slice input, geometry g64) ->
+// result in pr->gt(pr->coarse_res), n steps from t0.  Every kernel is gated by
+// item_lo against `item` when gate is set.
+int enqueue_coarse(sp_parareal* pr, const double* src, double t0, int n, bool gate, int item, cudaStream_t s) {
+    sp_convection* h = pr->prop;
+    const int cp = pr->cprec;
+    const Geo& gc = pr->gc;
+    const Tune t = h->tune(cp, 1);
+    int* err = h->err.as<int>();
+    const int* lo = gate ? pr->itemlo() : nullptr;
+    void* A = pr->gt(0);
+    void* B = pr->gt(1);
+    void* ya = pr->gt(2);
+    void* yb = pr->gt(3);
+    void* acc = pr->gt(4);
+    // bring the input into coarse precision / geometry
+    SP_CUDA(launch_convert(gc, A, pr->g64, src, s, lo, item));
+    void* cur = A;
+    void* other = B;
+    for (int i = 0; i < n; ++i) {
+        const double tt = i == 0 ? t0 : t0 + i * pr->dtC;
+        const NuSrc nu{computenu(h->P.nu0, h->P.nufreq, tt), nullptr};
+        if (pr->cfg.coarse_scheme == SP_COARSE_RK4) {
+            SP_CUDA(enqueue_rk4_step(gc, cp, h->coef, pr->dtC, nu, cur, cur, ya, yb, acc, 1, lo, item, t, s, err));
+        } else {
+            SP_CUDA(enqueue_euler_step(gc, cp, h->coef, pr->dtC, nu, cur, other, 1, lo, item, t, s, err));
+            std::swap(cur, other);
+        }
+    }
+    pr->coarse_res = (cur == A) ? 0 : 1;
+    return SP_OK;
+}
+
+// Captures one Parareal iteration (Parareal.h:116-165 for every slice):
+//   F sweep   : tsF RK4 steps of all slices r >= item_lo, batched per stage
+//   G sweep   : for r = item_lo..P-1: G(U_r) (coarse), correction into U_{r+1}
+int build_iteration_graph(sp_parareal* pr) {
+    sp_convection* h = pr->prop;
+    cudaStream_t s = h->stream();
+    const int P = pr->P;
+    const Geo& g = pr->g64;
+    const Tune tf = h->tune(0, P);
+    int* err = h->err.as<int>();
+    const size_t fstride = (size_t)P * g.total;
+    double* ya = pr->fs.as<double>();
+    double* yb = ya + fstride;
+    double* acc = yb + fstride;
+    const bool const_nu = h->P.nufreq == 0.;
+    SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const long long before = launches();
+    int rc = SP_OK;
+    cudaError_t e = cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal);
+    for (int i = 0; i < pr->tsF && e == cudaSuccess; ++i) {
+        NuSrc nu;
+        if (const_nu) nu.nu = h->P.nu0;
+        else nu.items = pr->nutab.as<double>() + (size_t)i * P;
+        const void* in = i == 0 ? (const void*)pr->u(0) : (const void*)pr->f(0);
+        e = enqueue_rk4_step(g, 0, h->coef, pr->dtF, nu, in, pr->f(0), ya, yb, acc, P, pr->itemlo(), 0, tf, s, err);
+    }
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
+    for (int r = 0; r < P && e == cudaSuccess && rc == SP_OK; ++r) {
+        const double tStart = pr->slice * r;
+        rc = enqueue_coarse(pr, pr->u(r), tStart, pr->tsC, true, r, s);
+        if (rc) break;
+        e = launch_update(g, pr->gc, pr->gt(pr->coarse_res), pr->f(r), pr->gold(r), pr->u(r + 1), pr->def() + 2 * r,
+                          pr->itemlo(), r, s);
+    }
+    if (e == cudaSuccess && rc == SP_OK) e = cudaEventRecordWithFlags(pr->ev[2], s, cudaEventRecordExternal);
+    const long long nodes = launches() - before;
+    add_launches(-nodes);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (rc != SP_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != SP_OK) return rc;
+        return fail(SP_ERR_CUDA, "iteration capture: %s", cudaGetErrorString(e));
+    }
+    if (e2 != cudaSuccess) return fail(SP_ERR_CUDA, "iteration end capture: %s", cudaGetErrorString(e2));
+    e = cudaGraphInstantiate(&pr->iter, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "iteration instantiate: %s", cudaGetErrorString(e));
+    pr->iter_nodes = nodes;
+    return SP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parareal** out) {
+    int rc = check_handle(prop);
+    if (rc) return rc;
+    if (!cfg || !out) return fail(SP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    const sp_parareal_cfg& c = *cfg;
+    if (c.timeSlices < 1 || c.timeStepsFine < 1 || c.timeStepsCoarse < 1 || c.kmax < 0 || !(c.endTime > 0))
+        return fail(SP_ERR_INVALID, "bad Parareal configuration");
+    if (c.kmax > SP_MAX_ITERS) return fail(SP_ERR_INVALID, "kmax > %d", SP_MAX_ITERS);
+    if (c.coarse_scheme != SP_COARSE_EULER && c.coarse_scheme != SP_COARSE_RK4)
+        return fail(SP_ERR_INVALID, "coarse_scheme");
+    if (c.coarse_precision != SP_F64 && c.coarse_precision != SP_F32) return fail(SP_ERR_INVALID, "coarse_precision");
+    std::unique_ptr<sp_parareal> pr(new sp_parareal());
+    pr->prop = prop;
+    pr->cfg = c;
+    const int P = c.timeSlices;
+    pr->P = P;
+    // RuntimeConfiguration.cpp:133-151: totals rounded up to a multiple of P.
+    int f = c.timeStepsFine, g = c.timeStepsCoarse;
+    if (f % P != 0) f = (f / P + 1) * P;
+    if (g % P != 0) g = (g / P + 1) * P;
+    pr->tsF = f / P;
+    pr->tsC = g / P;
+    pr->dtF = c.endTime / f;  // RuntimeConfiguration.h:54-65
+    pr->dtC = c.endTime / g;
+    pr->slice = c.endTime / P;
+    pr->cprec = c.coarse_precision == SP_F64 ? 0 : 1;
+    pr->g64 = prop->g[0];
+    pr->gc = prop->g[pr->cprec];
+    const size_t f64b = (size_t)pr->g64.total * 8;
+    const size_t cb = (size_t)pr->gc.total * pr->gc.es;
+    if (pr->U.alloc((P + 1) * f64b) != cudaSuccess || pr->F.alloc(P * f64b) != cudaSuccess ||
+        pr->fs.alloc(3 * P * f64b) != cudaSuccess || pr->Gold.alloc(P * cb) != cudaSuccess ||
+        pr->Gt.alloc(5 * cb) != cudaSuccess || pr->ctl.alloc(256 + (2 * P + 8) * sizeof(double)) != cudaSuccess)
+        return fail(SP_ERR_NOMEM, "Parareal state for %d slices", P);
+    if (prop->P.nufreq != 0.) {
+        // nu(t) per slice and fine step (Convection.h:81-84) with the time
+        // sequence of DoRK4 (Convection.cpp:296-302) or of the split first
+        // step of the asynchronous variant (Parareal.h:119-124).
+        std::vector<double> tab((size_t)pr->tsF * P);
+        for (int r = 0; r < P; ++r) {
+            const double tStart = pr->slice * r;
+            const double tStartFine = tStart + pr->dtF;
+            for (int i = 0; i < pr->tsF; ++i) {
+                double t;
+                if (c.async && r != 0) t = i == 0 ? tStart : (i == 1 ? tStartFine : tStartFine + (i - 1) * pr->dtF);
+                else t = i == 0 ? tStart : tStart + i * pr->dtF;
+                tab[(size_t)i * P + r] = computenu(prop->P.nu0, prop->P.nufreq, t);
+            }
+        }
+        if (pr->nutab.alloc(tab.size() * sizeof(double)) != cudaSuccess) return fail(SP_ERR_NOMEM, "nu table");
+        SP_CUDA(cudaMemcpy(pr->nutab.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    SP_CUDA(cudaMallocHost(&pr->h_itemlo, sizeof(int)));
+    SP_CUDA(cudaMallocHost(&pr->h_def, (2 * P + 8) * sizeof(double)));
+    for (auto& e : pr->ev) SP_CUDA(cudaEventCreate(&e));
+    *out = pr.release();
+    return SP_OK;
+}
+
+int sp_parareal_destroy(sp_parareal* pr) {
+    if (!pr) return SP_OK;
+    cudaSetDevice(pr->prop->device);
+    cudaStreamSynchronize(pr->prop->stream());
+    delete pr;
+    return SP_OK;
+}
+
+int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution) {
+    if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
+    // Parareal::DoSerial (Parareal.h:250-253)
+    return sp_do_rk4(pr->prop, initial, solution, 0., pr->dtF, pr->tsF * pr->P);
+}
+
+int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solution, const double* reference,
+                            sp_parareal_report* rep) {
+    if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
+    sp_convection* h = pr->prop;
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!initial || !solution) return fail(SP_ERR_INVALID, "null field");
+    cudaStream_t s = h->stream();
+    if (capturing(s)) return fail(SP_ERR_STATE, "DoParallel cannot run inside a stream capture");
+    const int P = pr->P;
+    const Geo& g = pr->g64;
+    const int cp = pr->cprec;
+    if ((rc = h->ensure_scratch(cp, 1))) return rc;
+    if (rep) {
+        std::memset(rep, 0, sizeof *rep);
+        rep->tsFine = pr->tsF; rep->tsCoarse = pr->tsC;
+        rep->dtFine = pr->dtF; rep->dtCoarse = pr->dtC; rep->timeSliceSize = pr->slice;
+    }
+    if (!pr->iter && (rc = build_iteration_graph(pr))) return rc;
+
+    SP_CUDA(cudaEventRecord(pr->ev[3], s));
+    // rank 0's qinitial is the initial field
+    SP_CUDA(cudaMemcpyAsync(pr->u(0), initial, g.total * 8, cudaMemcpyDeviceToDevice, s));
+    SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
+    // Predictor (Parareal.h:113-114).
+    const size_t cb = (size_t)pr->gc.total * pr->gc.es;
+    if (h->P.nufreq == 0.) {
+        // With constant nu, U_r = G^{tsC*r}(q0) from t=0 equals the chain
+        // U_{r+1} = G(U_r) step for step, and Gold_r = G(U_r) = U_{r+1}.
+        for (int r = 0; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(r), pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+            SP_CUDA(launch_convert(g, pr->u(r + 1), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+    } else {
+        for (int r = 1; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(0), 0., pr->tsC * r, false, 0, s))) return rc;
+            SP_CUDA(launch_convert(g, pr->u(r), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+        for (int r = 0; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(r), pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+            if (r == P - 1) SP_CUDA(launch_convert(g, pr->u(P), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+    }
+    // Iterations (Parareal.h:116-165).
+    int k = 0;
+    double t_f = 0., t_c = 0.;
+    long long fine_cu = 0;
+    const long long cells = (long long)g.ni * g.nj * g.nk;
+    for (; k < pr->cfg.kmax; ++k) {
+        const int lo = pr->cfg.skip_converged ? std::min(k, P) : 0;
+        *pr->h_itemlo = lo;
+        SP_CUDA(cudaMemcpyAsync(pr->itemlo(), pr->h_itemlo, sizeof(int), cudaMemcpyHostToDevice, s));
+        SP_CUDA(cudaGraphLaunch(pr->iter, s));
+        add_launches(pr->iter_nodes);
+        fine_cu += (long long)(P - lo) * pr->tsF * cells;
+        if (reference) {
+            SP_CUDA(cudaMemsetAsync(pr->err4(), 0, 4 * sizeof(double), s));
+            SP_CUDA(launch_errors(g, pr->u(P), reference, pr->err4(), s));
+        }
+        SP_CUDA(cudaMemcpyAsync(pr->h_def, pr->def(), (2 * P + 4) * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SP_CUDA(cudaStreamSynchronize(s));
+        float ms1 = 0, ms2 = 0;
+        cudaEventElapsedTime(&ms1, pr->ev[0], pr->ev[1]);
+        cudaEventElapsedTime(&ms2, pr->ev[1], pr->ev[2]);
+        t_f += ms1 * 1e-3;
+        t_c += ms2 * 1e-3;
+        double defect = 0.;
+        bool finite = true;
+        for (int r = lo; r < P; ++r) {
+            const double num = pr->h_def[2 * r], den = pr->h_def[2 * r + 1];
+            if (!std::isfinite(num) || !std::isfinite(den)) finite = false;
+            if (den > 0) defect = std::max(defect, std::sqrt(num / den));
+        }
+        double el2 = 0., emax = 0.;
+        if (reference) {
+            const double* e4 = pr->h_def + 2 * P;
+            el2 = std::sqrt(e4[0] / e4[1]);
+            emax = e4[2] / e4[3];
+        }
+        if (rep) {
+            rep->defect[k] = defect;
+            rep->err_l2[k] = el2;
+            rep->err_max[k] = emax;
+        }
+        if (!finite) {
+            if (rep) rep->iterations = k + 1;
+            return fail(SP_ERR_NONFINITE, "Parareal defect is not finite at iteration %d", k + 1);
+        }
+        if (pr->cfg.tol_kind == SP_TOL_DEFECT && defect < pr->cfg.tol) { ++k; break; }
+        if (pr->cfg.tol_kind == SP_TOL_REFERENCE && reference && el2 < pr->cfg.tol) { ++k; break; }
+    }
+    SP_CUDA(cudaMemcpyAsync(solution, pr->u(P), g.total * 8, cudaMemcpyDeviceToDevice, s));
+    SP_CUDA(cudaEventRecord(pr->ev[4], s));
+    SP_CUDA(cudaEventSynchronize(pr->ev[4]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, pr->ev[3], pr->ev[4]);
+    if (rep) {
+        rep->iterations = k;
+        rep->seconds = ms * 1e-3;
+        rep->seconds_fine = t_f;
+        rep->seconds_coarse = t_c;
+        rep->fine_cell_updates = fine_cu;
+    }
+    return sp_convection_synchronize(h);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of DoRK4 (Convection.cpp:292-370).  Per step, with h = dt, forward
+// stage inputs y1 = q, y2 = q + h/2 k1, y3 = q + h/2 k2, y4 = q + h k3 and the
+// step-end adjoint lam:
+//   mu4 = h/6 lam,               ybar4 = R^T mu4
+//   mu3 = h/3 lam + h   ybar4,   ybar3 = R^T mu3
+//   mu2 = h/3 lam + h/2 ybar3,   ybar2 = R^T mu2
+//   mu1 = h/6 lam + h/2 ybar2,   ybar1 = R^T mu1
+//   lam_prev = lam + ybar1 + ybar2 + ybar3 + ybar4
+//   dJ/dtheta += sum_s mu_s . dR/dtheta (y_s)
+// R^T is the same stencil with the velocity negated (D_d is antisymmetric
+// and Laplace4 symmetric on the periodic grid).  Checkpoints every `ck` steps;
+// each segment's stage inputs are recomputed and stored before its backward
+// sweep.
+extern "C" int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* q_target, const double* lambda_n,
+                              double tStart, double dt, int n, int ck, double* J, double* grad_q0,
+                              double* grad_par) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!q0 || !grad_q0 || (!q_target && !lambda_n)) return fail(SP_ERR_INVALID, "null field");
+    if (n < 0) return fail(SP_ERR_INVALID, "negative step count");
+    cudaStream_t s = h->stream();
+    if (capturing(s)) return fail(SP_ERR_STATE, "the adjoint cannot run inside a stream capture");
+    if (ck <= 0) ck = std::max(1, (int)std::ceil(std::sqrt((double)std::max(n, 1))));
+    ck = std::min(ck, std::max(n, 1));
+    const int nseg = n > 0 ? (n + ck - 1) / ck : 0;
+    const Geo& g = h->g[0];
+    const size_t fb = (size_t)g.total * 8;
+    if ((rc = h->ensure_scratch(0, 1))) return rc;
+    DevBuf ckpt, seg, work, par;
+    // work: qn, lam, lam_acc, mu_a, mu_b, dummy
+    if (ckpt.alloc(std::max(nseg, 1) * fb) != cudaSuccess || seg.alloc((size_t)4 * ck * fb) != cudaSuccess ||
+        work.alloc(6 * fb) != cudaSuccess || par.alloc(8 * sizeof(double)) != cudaSuccess)
+        return fail(SP_ERR_NOMEM, "adjoint buffers (%d checkpoints, %d-step segments)", nseg, ck);
+    auto CK = [&](int i) { return ckpt.as<double>() + (size_t)i * g.total; };
+    auto SG = [&](int i) { return seg.as<double>() + (size_t)i * g.total; };  // [y2 | y3 | y4 | state] x ck
+    auto WK = [&](int i) { return work.as<double>() + (size_t)i * g.total; };
+    double* qn = WK(0);
+    double* lam = WK(1);
+    double* lamacc = WK(2);
+    double* mua = WK(3);
+    double* mub = WK(4);
+    double* dummy = WK(5);
+    const Tune t = h->tune(0, 1);
+    int* err = h->err.as<int>();
+    double* ya = static_cast<double*>(h->sbuf(0, 0, 1));
+    double* yb = static_cast<double*>(h->sbuf(0, 1, 1));
+    double* acc = static_cast<double*>(h->sbuf(0, 2, 1));
+    const double nu0 = h->P.nu0, nuf = h->P.nufreq;
+    SP_CUDA(cudaMemsetAsync(par.p, 0, 8 * sizeof(double), s));
+    // forward sweep, keeping checkpoints
+    SP_CUDA(cudaMemcpyAsync(nseg > 0 ? CK(0) : qn, q0, fb, cudaMemcpyDeviceToDevice, s));
+    SP_CUDA(launch_periodicity(g, nseg > 0 ? CK(0) : qn, 1, s));
+    for (int sg = 0; sg < nseg; ++sg) {
+        const int s0 = sg * ck, s1 = std::min(n, s0 + ck);
+        double* dst = (sg + 1 < nseg) ? CK(sg + 1) : qn;
+        for (int st = s0; st < s1; ++st) {
+            const double tt = tStart + st * dt;
+            SP_CUDA(enqueue_rk4_step(g, 0, h->coef, dt, NuSrc{computenu(nu0, nuf, tt), nullptr},
+                                     st == s0 ? (const void*)CK(sg) : (const void*)dst, dst, ya, yb, acc, 1, nullptr,
+                                     0, t, s, err));
+        }
+    }
+    // terminal adjoint
+    if (lambda_n) {
+        SP_CUDA(cudaMemcpyAsync(lam, lambda_n, fb, cudaMemcpyDeviceToDevice, s));
+        SP_CUDA(launch_periodicity(g, lam, 1, s));
+    } else {
+        SP_CUDA(launch_misfit(g, qn, q_target, lam, par.as<double>() + 4, s));
+    }
+    // backward sweep
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int s0 = sg * ck, s1 = std::min(n, s0 + ck), m = s1 - s0;
+        auto Y2 = [&](int i) { return SG(4 * i + 0); };
+        auto Y3 = [&](int i) { return SG(4 * i + 1); };
+        auto Y4 = [&](int i) { return SG(4 * i + 2); };
+        auto ST = [&](int i) { return i == 0 ? CK(sg) : SG(4 * (i - 1) + 3); };  // state at step s0+i
+        for (int i = 0; i < m; ++i) {
+            const double tt = tStart + (s0 + i) * dt;
+            double* next = (i + 1 < m) ? SG(4 * i + 3) : dummy;
+            SP_CUDA(enqueue_rk4_step3(g, 0, h->coef, dt, NuSrc{computenu(nu0, nuf, tt), nullptr}, ST(i), next, Y2(i),
+                                      Y3(i), Y4(i), acc, 1, nullptr, 0, t, s, err));
+        }
+        for (int i = m - 1; i >= 0; --i) {
+            const double tt = tStart + (s0 + i) * dt;
+            StageLaunch L;
+            L.prec = 0;
+            L.items = 1;
+            L.coef = h->coef;
+            L.nu = computenu(nu0, nuf, tt);
+            L.dnu = 1. + .5 * std::sin(nuf * tt);
+            L.par_acc = par.as<double>();
+            // A4: stencil lam (mu4 = h/6 lam)
+            L.op = OP_ADJ + 0; L.yin = lam; L.sigma = dt / 6.; L.ypt = Y4(i);
+            L.yout = mua; L.lam_acc = lamacc; L.c_ybar = dt; L.c_lam = dt / 3.;
+            SP_CUDA(launch_stage(g, L, t, s, err));
+            // A3: stencil mu3
+            L.op = OP_ADJ + 1; L.yin = mua; L.sigma = 1.; L.ypt = Y3(i); L.lam = lam;
+            L.yout = mub; L.c_ybar = dt * .5; L.c_lam = dt / 3.;
+            SP_CUDA(launch_stage(g, L, t, s, err));
+            // A2: stencil mu2
+            L.op = OP_ADJ + 2; L.yin = mub; L.ypt = Y2(i);
+            L.yout = mua; L.c_ybar = dt * .5; L.c_lam = dt / 6.;
+            SP_CUDA(launch_stage(g, L, t, s, err));
+            // A1: stencil mu1 -> lam_prev (with images)
+            L.op = OP_ADJ + 3; L.yin = mua; L.ypt = ST(i); L.yout = lamacc;
+            SP_CUDA(launch_stage(g, L, t, s, err));
+            std::swap(lam, lamacc);
+        }
+    }
+    SP_CUDA(cudaMemcpyAsync(grad_q0, lam, fb, cudaMemcpyDeviceToDevice, s));
+    double hp[8];
+    SP_CUDA(cudaMemcpyAsync(hp, par.p, sizeof hp, cudaMemcpyDeviceToHost, s));
+    if ((rc = sp_convection_synchronize(h))) return rc;
+    if (grad_par) for (int i = 0; i < 4; ++i) grad_par[i] = hp[i];
+    if (J) *J = lambda_n ? 0. : hp[4];
+    return SP_OK;
+}

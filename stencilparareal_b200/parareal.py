@@ -1,0 +1,161 @@
+"""Python mirror of the reference's Parareal driver and its configuration.
+
+``RuntimeConfiguration`` keeps the getters, defaults and step rounding of
+src/Parareal/RuntimeConfiguration.{h,cpp} (defaults RuntimeConfiguration.cpp:7-13,
+rounding :133-151, derived values RuntimeConfiguration.h:54-111); the number of
+time slices, which the reference takes from the MPI communicator size
+(RuntimeConfiguration.cpp:15), is an explicit argument here.
+
+``Parareal`` follows template class Parareal (src/Parareal/Parareal.h:38-289):
+constructed from a propagator, the initial and solution fields, the start
+time and a configuration; ``DoParallel`` and ``DoSerial`` keep their meaning.
+All P slices run on one GPU inside ``libstencilparareal.so``: the fine runs of
+all slices are batched per RK stage, the coarse sweep runs slice by slice and
+the correction writes straight into the next slice's input, which replaces
+the MPI ring of Parareal.h:122-162.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+from . import _lib as L
+from .convection import Convection, ConvectionField
+
+MODES = ("compare", "serial", "parallel", "timing")
+
+
+class RuntimeConfiguration:
+    def __init__(self, timeSlices: int = 1, nu0: float = 1.0, nufreq: float = 0.0, cx: float = 1.0,
+                 cy: float = 1.0, cz: float = 1.0, gridSize: int = 32, endTime: float = 0.05,
+                 timeStepsFine: int = 128, timeStepsCoarse: int = 32, kmax: int = 5, mat: bool = False,
+                 async_: bool = True, mode: str = "compare"):
+        if timeSlices < 1:
+            raise ValueError("timeSlices must be >= 1")
+        self._nu0, self._nufreq = nu0, nufreq
+        self._cx, self._cy, self._cz = cx, cy, cz
+        self._gridSize, self._endTime = gridSize, endTime
+        self._timeSlices = timeSlices
+        self._kmax, self._mat, self._async = kmax, mat, async_
+        m = mode.lower()
+        self._mode = m if m in MODES else "compare"  # unknown modes fall back to Compare (RuntimeConfiguration.cpp:125-130)
+        # RuntimeConfiguration.cpp:133-151: round totals up to a multiple of the slice count
+        if timeStepsFine % timeSlices != 0:
+            timeStepsFine = (timeStepsFine // timeSlices + 1) * timeSlices
+        if timeStepsCoarse % timeSlices != 0:
+            timeStepsCoarse = (timeStepsCoarse // timeSlices + 1) * timeSlices
+        self._timeStepsFine, self._timeStepsCoarse = timeStepsFine, timeStepsCoarse
+
+    # getters (RuntimeConfiguration.h:19-31)
+    def nu0(self): return self._nu0
+    def nufreq(self): return self._nufreq
+    def cx(self): return self._cx
+    def cy(self): return self._cy
+    def cz(self): return self._cz
+    def timeSlices(self): return self._timeSlices
+    def timeStepsFine(self): return self._timeStepsFine
+    def timeStepsCoarse(self): return self._timeStepsCoarse
+    def gridSize(self): return self._gridSize
+    def endTime(self): return self._endTime
+    def kmax(self): return self._kmax
+    def mat(self): return self._mat
+    def async_(self): return self._async
+    def mode(self): return self._mode
+
+    # derived (RuntimeConfiguration.h:54-111)
+    def dx(self): return 1.0 / self._gridSize
+    def dtFine(self): return self._endTime / self._timeStepsFine
+    def dtCoarse(self): return self._endTime / self._timeStepsCoarse
+    def timeStepsFinePerTimeSlice(self): return self._timeStepsFine // self._timeSlices
+    def timeStepsCoarsePerTimeSlice(self): return self._timeStepsCoarse // self._timeSlices
+    def timeSliceSize(self): return self._endTime / self._timeSlices
+    def cflFine(self): return self._cfl(self.dtFine())
+    def cflCoarse(self): return self._cfl(self.dtCoarse())
+
+    def _cfl(self, dt):
+        c = max(self._cx, self._cy, self._cz)
+        dt_dx = dt / self.dx()
+        return max(1.5 * self._nu0 * dt_dx / self.dx(), c * dt_dx)
+
+
+class Parareal:
+    """template class Parareal (Parareal.h:38-289), all slices on one GPU.
+
+    Extra knobs beyond the reference: ``coarse`` ('euler' = the reference's
+    DoEuler, or 'rk4'), ``coarse_precision`` ('f64' or 'f32'), a stopping
+    tolerance ``tol`` on the relative L2 defect (``tol_kind='defect'``) or on
+    the error against a given reference field (``tol_kind='reference'``), and
+    ``skip_converged`` (slices < k are exact after k iterations; their fine
+    runs are skipped -- the results are bit-identical).
+    """
+
+    def __init__(self, propagator: Convection, initial: ConvectionField, solution: ConvectionField,
+                 tStart: float, conf: RuntimeConfiguration, coarse: str = "euler", coarse_precision: str = "f64",
+                 tol: float = 0.0, tol_kind: str = "none", skip_converged: bool = True):
+        self.prop = propagator
+        self.initial = initial
+        self.solution = solution
+        self.tStart = tStart
+        self.conf = conf
+        cfg = L.SpPararealCfg()
+        cfg.endTime = conf.endTime()
+        cfg.timeSlices = conf.timeSlices()
+        cfg.timeStepsFine = conf.timeStepsFine()
+        cfg.timeStepsCoarse = conf.timeStepsCoarse()
+        cfg.kmax = int(conf.kmax())
+        cfg.async_ = 1 if conf.async_() else 0
+        cfg.coarse_scheme = {"euler": L.SP_COARSE_EULER, "rk4": L.SP_COARSE_RK4}[coarse]
+        cfg.coarse_precision = {"f64": L.SP_F64, "f32": L.SP_F32}[coarse_precision]
+        cfg.tol_kind = {"none": L.SP_TOL_NONE, "defect": L.SP_TOL_DEFECT, "reference": L.SP_TOL_REFERENCE}[tol_kind]
+        cfg.tol = tol
+        cfg.skip_converged = 1 if skip_converged else 0
+        self.cfg = cfg
+        h = C.c_void_p()
+        L.check(L.lib().sp_parareal_create(propagator.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            L.lib().sp_parareal_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def DoParallel(self, reference: ConvectionField | None = None) -> dict:
+        """Parareal::DoParallel (Parareal.h:110-171); returns the run report."""
+        rep = L.SpPararealReport()
+        ref = C.c_void_p(reference.ptr) if reference is not None else None
+        self.prop.call(L.lib().sp_parareal_do_parallel, self._h, C.c_void_p(self.initial.ptr),
+                       C.c_void_p(self.solution.ptr), ref, C.byref(rep))
+        k = rep.iterations
+        return {"iterations": k, "tsFine": rep.tsFine, "tsCoarse": rep.tsCoarse, "dtFine": rep.dtFine,
+                "dtCoarse": rep.dtCoarse, "timeSliceSize": rep.timeSliceSize,
+                "defect": list(rep.defect[:k]), "err_l2": list(rep.err_l2[:k]), "err_max": list(rep.err_max[:k]),
+                "seconds": rep.seconds, "seconds_fine": rep.seconds_fine, "seconds_coarse": rep.seconds_coarse,
+                "fine_cell_updates": rep.fine_cell_updates}
+
+    def DoSerial(self):
+        """Parareal::DoSerial (Parareal.h:250-253)."""
+        self.prop.call(L.lib().sp_parareal_do_serial, self._h, C.c_void_p(self.initial.ptr),
+                       C.c_void_p(self.solution.ptr))
+
+    @staticmethod
+    def max_speedup(tau_ratio: float, kmax: int, slices: int) -> float:
+        """The reference's speedup model (src/Parareal/main.cpp:208-210)."""
+        nit_np = kmax / slices
+        return 1.0 / (tau_ratio * (1.0 + nit_np) + nit_np)
+
+
+def slice_bounds(P: int, world: int, rank: int):
+    """Contiguous slice range [lo, hi) of rank `rank` when P slices are spread over `world` GPUs."""
+    base, extra = divmod(P, world)
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
+def cfl_ok(conf: RuntimeConfiguration) -> bool:
+    return math.isfinite(conf.cflFine())

@@ -1,0 +1,100 @@
+"""GPU Parareal (all slices on one GPU) against the oracle's serial restatement
+of Parareal::DoSerial + DoParallel (Parareal.h:110-171,250-253)."""
+import numpy as np
+import pytest
+
+from ics import gaussian_noise, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+COARSE = {
+    ("euler", "f64"): 0, ("rk4", "f64"): 1, ("rk4", "f32"): 2, ("euler", "f32"): 3,
+}
+
+
+def setup(sp, orc, n, P, kmax, coarse, prec, nu0=0.05, nufreq=0.0, T=0.02, tsF=160, tsC=12, async_=False,
+          skip=True, seed=0):
+    conv = sp.Convection(n, n, n, 1.0 / n, nu0, nufreq, 1.0, 0.5, -0.25)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, nufreq=nufreq, gridSize=n, endTime=T,
+                                   timeStepsFine=tsF, timeStepsCoarse=tsC, kmax=kmax, async_=async_)
+    q0 = gaussian_noise(n, seed=seed)
+    fin, fsol, fref = conv.field(), conv.field(), conv.field()
+    conv.upload(fin, q0)
+    par = sp.Parareal(conv, fin, fsol, 0.0, conf, coarse=coarse, coarse_precision=prec, skip_converged=skip)
+    p = orc.params(n, nu0=nu0, nufreq=nufreq, cx=1.0, cy=0.5, cz=-0.25)
+    cfg = orc.parareal_cfg(T, P, tsF, tsC, kmax, async_=async_, coarse=COARSE[(coarse, prec)])
+    return conv, par, fin, fsol, fref, p, cfg, q0
+
+
+@pytest.mark.parametrize("coarse,prec", list(COARSE))
+def test_parareal_matches_oracle(sp, orc, coarse, prec):
+    n, P, kmax = 16, 4, 3
+    conv, par, fin, fsol, fref, p, cfg, q0 = setup(sp, orc, n, P, kmax, coarse, prec)
+    # serial fine reference on the GPU (DoSerial) and on the oracle
+    ser = sp.Parareal(conv, fin, fref, 0.0, par.conf, coarse=coarse, coarse_precision=prec)
+    ser.DoSerial()
+    rep = par.DoParallel(reference=fref)
+    qo, qs, em, el = orc.parareal(p, cfg, q0)
+    assert rel_l2(conv.download(fref), qs) < 1e-12
+    # FP64 coarse: rounding-level agreement.  FP32 coarse: G's FP32 rounding
+    # (FMA contraction and operand order differ from the oracle's literal FP32
+    # order) stays in the iterate until the slices converge, ~1e-7 relative.
+    tol = 1e-11 if prec == "f64" else 1e-6
+    assert rel_l2(conv.download(fsol), qo) < tol
+    assert rep["iterations"] == kmax
+    for k in range(kmax):
+        # per-iteration errors against the serial solution agree with the oracle's
+        if prec == "f64":
+            assert abs(rep["err_max"][k] - em[k]) <= 1e-6 * em[k] + 1e-13, (k, rep["err_max"][k], em[k])
+        else:
+            assert abs(rep["err_max"][k] - em[k]) <= 0.05 * em[k] + 1e-6, (k, rep["err_max"][k], em[k])
+
+
+def test_exact_after_P_iterations_and_skip_is_bitwise(sp, orc):
+    n, P = 12, 4
+    outs = []
+    for skip in (True, False):
+        conv, par, fin, fsol, fref, p, cfg, q0 = setup(sp, orc, n, P, P, "rk4", "f32", skip=skip)
+        ser = sp.Parareal(conv, fin, fref, 0.0, par.conf)
+        ser.DoSerial()
+        rep = par.DoParallel(reference=fref)
+        assert rep["err_l2"][-1] < 1e-14, rep["err_l2"]
+        outs.append(conv.download(fsol))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_time_dependent_nu_and_async_sequence(sp, orc):
+    n, P, kmax = 12, 3, 2
+    for async_ in (False, True):
+        conv, par, fin, fsol, fref, p, cfg, q0 = setup(sp, orc, n, P, kmax, "euler", "f64", nufreq=100.0,
+                                                       async_=async_)
+        par.DoParallel()
+        qo, qs, em, el = orc.parareal(p, cfg, q0)
+        assert rel_l2(conv.download(fsol), qo) < 1e-11
+
+
+def test_rounding_and_report(sp, orc):
+    n, P = 8, 32
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.01, gridSize=n, endTime=0.2, timeStepsFine=20000,
+                                   timeStepsCoarse=200, kmax=1)
+    f0, f1 = conv.field(), conv.field()
+    conv.upload(f0, gaussian_noise(n))
+    par = sp.Parareal(conv, f0, f1, 0.0, conf, coarse="rk4", coarse_precision="f32")
+    rep = par.DoParallel()
+    assert rep["tsFine"] == 625 and rep["tsCoarse"] == 7
+    assert abs(rep["dtCoarse"] - 0.2 / 224) < 1e-18
+    assert rep["fine_cell_updates"] == 32 * 625 * n ** 3
+
+
+def test_tolerance_stops_early(sp, orc):
+    n, P = 12, 8
+    conv, par, fin, fsol, fref, p, cfg, q0 = setup(sp, orc, n, P, 8, "rk4", "f64")
+    ser = sp.Parareal(conv, fin, fref, 0.0, par.conf)
+    ser.DoSerial()
+    par2 = sp.Parareal(conv, fin, fsol, 0.0, par.conf, coarse="rk4", coarse_precision="f64", tol=1e-8,
+                       tol_kind="reference")
+    rep = par2.DoParallel(reference=fref)
+    assert rep["iterations"] < 8
+    assert rep["err_l2"][-1] < 1e-8
+    assert all(e >= 1e-8 for e in rep["err_l2"][:-1])
