@@ -188,6 +188,26 @@ int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* q_target, c
                    double tStart, double dt, int n, int checkpoint_every, double* J, double* grad_q0,
                    double* grad_par);
 
+/* ---- allocation-free propagation ---------------------------------------------- */
+/* No counterpart in the reference: an extra entry point of this library.
+ * DoRK4 (same stepping and result as sp_do_rk4) for callers that cannot call
+ * cudaMalloc -- e.g. code running inside a process whose GPU memory belongs
+ * to another allocator or is fully reserved up front, or a plugin that may
+ * only touch the buffers it is given.  It needs no handle and allocates
+ * nothing: the three RK4 work fields live in a device array built into the
+ * library, SP_NOALLOC_SCRATCH_BYTES on every GPU that loads it, held until the
+ * process exits.  Grids whose three FP64 work fields do not fit (beyond about
+ * 80^3) are rejected with SP_ERR_INVALID.  `in`/`out` are FP64 fields in the
+ * sp_field_layout geometry on the current device; the call runs on `stream`
+ * (NULL = legacy default stream) and returns when the steps are done.  The
+ * first call on each device looks up the array's device address and sets the
+ * kernels' shared-memory limits; make that first call before any stream
+ * capture.  All calls share the one array: calls whose GPU work overlaps
+ * (other streams, other host threads) race on it. */
+#define SP_NOALLOC_SCRATCH_BYTES (16u << 20)
+int sp_do_rk4_noalloc(const sp_params* p, const double* in, double* out, double tStart, double dt, int timesteps,
+                      void* stream);
+
 /* ---- misc ------------------------------------------------------------------- */
 const char* sp_last_error(void);
 int sp_abi_version(void);

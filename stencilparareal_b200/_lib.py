@@ -28,6 +28,7 @@ SP_TOL_NONE = 0
 SP_TOL_DEFECT = 1
 SP_TOL_REFERENCE = 2
 SP_MAX_ITERS = 64
+SP_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class SpParams(C.Structure):
@@ -96,6 +97,7 @@ _SIGS = {
     "sp_tuned_config": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "sp_autotune": (_i, [_vp, _i, _i]),
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
+    "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),
 }
 
 

@@ -101,4 +101,7 @@ cudaError_t launch_misfit(const Geo& g, const double* a, const double* b, double
 long long launches();
 void add_launches(long long n);
 
+// Records `fmt` as the calling thread's last error (sp_last_error) and returns code.
+int sp_report(int code, const char* fmt, ...);
+
 }  // namespace sp

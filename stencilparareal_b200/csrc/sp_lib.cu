@@ -70,6 +70,16 @@ struct DevBuf {
 
 }  // namespace
 
+int sp::sp_report(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
 // ---------------------------------------------------------------------------
 // Propagator handle.
 struct GraphEntry {
