@@ -212,6 +212,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-parareal", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", default="auto", help="'auto' or ty,zchunk,kind for the stage kernels")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: one 256^3 DoRK4 of 2 steps with the given --tune, no timing")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -234,10 +237,20 @@ def main():
     torch.cuda.set_device(device)
     n = N_FINE
     conv = sp.Convection(n, n, n, 1.0 / n, NU, 0.0, C[0], C[1], C[2], device=device)
-    tune = conv.autotune(sp.SP_F64, 1)
+    if args.tune == "auto" and not args.profile:
+        tune = conv.autotune(sp.SP_F64, 1)
+    else:
+        ty, zc, kind = (int(x) for x in (args.tune if args.tune != "auto" else "4,8,1").split(","))
+        conv.set_tune(sp.SP_F64, 1, ty, zc, kind)
+        tune = conv.tuned_config(sp.SP_F64, 1)
     q0 = fourier_ic(n)
     fin, fout = conv.field(), conv.field()
     conv.upload(fin, q0)
+    if args.profile:
+        conv.DoRK4(fin, fout, 0.0, DT, 2)
+        conv.synchronize()
+        print(json.dumps({"profile": WORKLOAD.replace(f"x {STEPS_PER_RUN} steps", "x 2 steps"), "tune": tune}))
+        return 0
     stream = conv.stream
 
     def one_step():

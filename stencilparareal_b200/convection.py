@@ -183,8 +183,9 @@ class Convection:
         return out
 
     # -- tuning ----------------------------------------------------------------
-    def set_tune(self, precision: int, batch: int, ty: int, zchunk: int, tma: bool):
-        L.check(L.lib().sp_set_tune(self._h, precision, batch, ty, zchunk, 1 if tma else 0))
+    def set_tune(self, precision: int, batch: int, ty: int, zchunk: int, kind: int):
+        """kind: 0 direct loads, 1 TMA/mbarrier pipeline."""
+        L.check(L.lib().sp_set_tune(self._h, precision, batch, ty, zchunk, int(kind)))
 
     def autotune(self, precision: int = L.SP_F64, batch: int = 1):
         self.call(L.lib().sp_autotune, self._h, precision, batch)
@@ -193,7 +194,7 @@ class Convection:
     def tuned_config(self, precision: int = L.SP_F64, batch: int = 1):
         ty, zc, tma = C.c_int(), C.c_int(), C.c_int()
         L.check(L.lib().sp_tuned_config(self._h, precision, batch, C.byref(ty), C.byref(zc), C.byref(tma)))
-        return {"ty": ty.value, "zchunk": zc.value, "tma": bool(tma.value)}
+        return {"ty": ty.value, "zchunk": zc.value, "kind": tma.value}
 
 
 def launch_count() -> int:

@@ -29,8 +29,8 @@ enum Op : int {
 
 // Launch-shape choice for the stage kernels.
 struct Tune {
-    int ty = 8;       // rows of a CTA tile (warps per CTA for the TMA kernel)
-    int zchunk = 32;  // planes marched by one CTA
+    int ty = 8;       // rows of a CTA tile
+    int zchunk = 32;  // planes of one work item (a CTA's z-march)
     int tma = 1;      // 1: TMA/mbarrier pipeline kernel; 0: direct-load kernel
 };
 

@@ -86,6 +86,13 @@ Coef make_coef(double dx, double cx, double cy, double cz, int upwind) {
 }
 
 // ---------------------------------------------------------------------------
+// R4 as 13 per-offset weights of the reference's coefficients:
+//   ca_d (8(q[-1]-q[+1]) - (q[-2]-q[+2])) + nl (16 S1 - S2 - 90 q).
+template <typename T>
+struct W13 {
+    T m1[3], p1[3], m2[3], p2[3], c;
+};
+
 // Kernel arguments.
 template <typename T>
 struct KArgs {
@@ -110,6 +117,7 @@ struct KArgs {
     T sigma;                  // adjoint: mu_s = sigma * (stencil input)
     double* par_acc;          // adjoint: 4 parameter-gradient sums
     double gs_nu, gs_c;       // adjoint: scales of the nu and c sums
+    W13<T> w;                 // RHS4 weights for the launch's nu (TMA RK stages)
     int* err;
 };
 
@@ -306,7 +314,19 @@ __global__ void __launch_bounds__(32 * TYD) k_stage_direct(const KArgs<T> a) {
 // TMA stage kernel.  Block = 32*TY threads (warp w owns tile row w), grid
 // (tiles_x*tiles_y, nzc, items).  Shared memory: NS stencil-input slots of
 // (TX+2LX) x (TY+4) elements and NP pointwise slots of npw x TX x TY elements,
-// followed by NS+NP mbarriers.
+// followed by NS+NP mbarriers.  Ring bookkeeping uses running slot indices
+// and phase bits instead of divisions; CTAs whose tile is two or more cells
+// away from every x/y face skip the periodic-image logic except on the four
+// planes next to the z faces.
+
+template <typename T>
+__device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
+    const T sx = fmaT(w.m2[0], s.xm2, fmaT(w.m1[0], s.xm1, fmaT(w.p1[0], s.xp1, w.p2[0] * s.xp2)));
+    const T sy = fmaT(w.m2[1], s.ym2, fmaT(w.m1[1], s.ym1, fmaT(w.p1[1], s.yp1, w.p2[1] * s.yp2)));
+    const T sz = fmaT(w.m2[2], s.zm2, fmaT(w.m1[2], s.zm1, fmaT(w.p1[2], s.zp1, w.p2[2] * s.zp2)));
+    return fmaT(w.c, s.c, (sx + sy) + sz);
+}
+
 template <typename T, int OP, int TY, int NS, int NP>
 __global__ void __launch_bounds__(32 * TY)
     k_stage_tma(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_p0,
@@ -322,7 +342,9 @@ __global__ void __launch_bounds__(32 * TY)
     constexpr int NPA = OpTraits<OP>::npw;
     constexpr uint32_t YBYTES = YT * sizeof(T);
     constexpr uint32_t PBYTES = NPA * PT * sizeof(T);
+    constexpr bool RK = OP <= OP_RK_S4;
     static_assert((YT * sizeof(T)) % 128 == 0 && (PT * sizeof(T)) % 128 == 0, "slot alignment");
+    static_assert(NS >= 4, "ring depth");
     using V = Vec<T, VX>;
 
     extern __shared__ unsigned char smem_raw[];
@@ -354,8 +376,7 @@ __global__ void __launch_bounds__(32 * TY)
 
     // tile t (interior plane, z0-2 <= t <= z1+1) -> slot (t - z0 + 2) % NS
     auto issue_y = [&](int t) {
-        const int u = t - z0 + 2;
-        const int s = u % NS;
+        const int s = (t - z0 + 2) % NS;
         mbar_arrive_expect_tx(&bar[s], YBYTES);
         tma_load_3d(ys + s * YT, &tm_s, x0, y0, zb + t, &bar[s]);
     };
@@ -374,14 +395,18 @@ __global__ void __launch_bounds__(32 * TY)
             for (int t = z0; t < z0 + NP && t < z1; ++t) { issue_p(t); p_hi = t; }
     }
 
+    // running ring positions: slot and phase of stencil tile z+2 (the next
+    // centre), of tile z (x/y neighbours) and of pointwise tile z
+    int s_c = 0;
+    uint32_t ph_c = 0;
     bool bad = false;
-    auto center = [&](int t) -> V {
-        const int u = t - z0 + 2;
-        const int s = u % NS;
-        if (!mbar_wait_bounded(&bar[s], (uint32_t)((u / NS) & 1))) bad = true;
-        return ld16<T>(ys + s * YT + (w + 2) * W + LX + lane * VX);
+    const int own = (w + 2) * W + LX + lane * VX;  // this thread's centre in a stencil tile
+    auto next_center = [&]() -> V {
+        if (!mbar_wait_bounded(&bar[s_c], ph_c)) bad = true;
+        const V v = ld16<T>(ys + s_c * YT + own);
+        if (++s_c == NS) { s_c = 0; ph_c ^= 1u; }
+        return v;
     };
-    // Leader-only drain of copies still in flight, before an early return.
     auto drain = [&](int y_done, int p_done) {
         if (!leader) return;
         for (int t = y_done + 1; t <= y_hi; ++t) {
@@ -392,7 +417,7 @@ __global__ void __launch_bounds__(32 * TY)
             (void)mbar_wait_bounded(&bar[NS + (t - z0) % NP], (uint32_t)(((t - z0) / NP) & 1));
     };
 
-    V cm2 = center(z0 - 2), cm1 = center(z0 - 1), c0 = center(z0), cp1 = center(z0 + 1);
+    V cm2 = next_center(), cm1 = next_center(), c0 = next_center(), cp1 = next_center();
     if (__syncthreads_or(bad)) {
         if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         drain(z0 + 1, z0 - 1);
@@ -405,21 +430,32 @@ __global__ void __launch_bounds__(32 * TY)
 
     const T nl = item_nl(a, b);
     const int y = y0 + w;
+    const int x = x0 + lane * VX;
+    const bool live = y < a.nj && x < a.ni;
+    const bool full_vec = x + VX <= a.ni;
+    const bool img_xy = x0 < 2 || x0 + TX > a.ni - 2 || y0 < 2 || y0 + TY > a.nj - 2;
     const long long ob = (long long)b * a.item_stride + a.origin;
+    T* yrow_out = a.yout + ob + (long long)z0 * a.plane + (long long)y * a.px + x;
+    T* arow_out = nullptr;
+    if constexpr (OpTraits<OP>::writes_a) arow_out = a.aout + ob + (long long)z0 * a.plane + (long long)y * a.px + x;
     double g[4] = {0., 0., 0., 0.};
+    int s_n = 2 % NS;  // slot of tile z (neighbours)
+    int s_p = 0;
+    uint32_t ph_p = 0;
 
     for (int z = z0; z < z1; ++z) {
-        const V cp2 = center(z + 2);
+        const V cp2 = next_center();
         V p0v, p1v, p2v;
         if constexpr (NPA > 0) {
-            const int s = (z - z0) % NP;
-            if (!mbar_wait_bounded(&bar[NS + s], (uint32_t)(((z - z0) / NP) & 1))) bad = true;
-            const T* P = ps + s * NPA * PT + w * TX + lane * VX;
+            if (!mbar_wait_bounded(&bar[NS + s_p], ph_p)) bad = true;
+            const T* P = ps + s_p * NPA * PT + w * TX + lane * VX;
             p0v = ld16<T>(P);
             if constexpr (NPA > 1) p1v = ld16<T>(P + PT);
             if constexpr (NPA > 2) p2v = ld16<T>(P + 2 * PT);
+            if (++s_p == NP) { s_p = 0; ph_p ^= 1u; }
         }
-        const T* Y = ys + ((z - z0 + 2) % NS) * YT;
+        const T* Y = ys + s_n * YT;
+        if (++s_n == NS) s_n = 0;
         T row[3 * VX];
         {
             const T* R = Y + (w + 2) * W + lane * VX;
@@ -427,9 +463,9 @@ __global__ void __launch_bounds__(32 * TY)
 #pragma unroll
             for (int e = 0; e < VX; ++e) { row[e] = r0.v[e]; row[VX + e] = r1.v[e]; row[2 * VX + e] = r2.v[e]; }
         }
-        const T* C = Y + LX + lane * VX;
-        const V ym2 = ld16<T>(C + w * W), ym1 = ld16<T>(C + (w + 1) * W);
-        const V yp1 = ld16<T>(C + (w + 3) * W), yp2 = ld16<T>(C + (w + 4) * W);
+        const T* Cn = Y + LX + lane * VX;
+        const V ym2 = ld16<T>(Cn + w * W), ym1 = ld16<T>(Cn + (w + 1) * W);
+        const V yp1 = ld16<T>(Cn + (w + 3) * W), yp2 = ld16<T>(Cn + (w + 4) * W);
         V oy, oa;
 #pragma unroll
         for (int e = 0; e < VX; ++e) {
@@ -444,15 +480,33 @@ __global__ void __launch_bounds__(32 * TY)
             if constexpr (NPA > 1) q1 = p1v.v[e];
             if constexpr (NPA > 2) q2 = p2v.v[e];
             T vy = 0, va = 0;
-            cell_op<T, OP>(a, nl, s, q0, q1, q2, vy, va, g, y < a.nj && x0 + lane * VX + e < a.ni);
+            if constexpr (RK) {
+                const T k = rhs_w13(a.w, s);
+                if constexpr (OP == OP_RK_S1) {
+                    vy = fmaT(a.c_y, k, s.c);
+                    va = fmaT(a.c_acc, k, s.c);
+                } else if constexpr (OP == OP_RK_S2 || OP == OP_RK_S3) {
+                    vy = fmaT(a.c_y, k, q0);
+                    va = fmaT(a.c_acc, k, q1);
+                } else {
+                    vy = fmaT(a.c_acc, k, q0);
+                }
+            } else {
+                cell_op<T, OP>(a, nl, s, q0, q1, q2, vy, va, g, live && x + e < a.ni);
+            }
             oy.v[e] = vy;
             oa.v[e] = va;
         }
-        const int x = x0 + lane * VX;
-        if (y < a.nj && x < a.ni) {
-            store_images_vec<T, VX>(a.yout + ob, x, y, z, oy, a, true);
-            if constexpr (OpTraits<OP>::writes_a) store_images_vec<T, VX>(a.aout + ob, x, y, z, oa, a, false);
+        if (live) {
+            if (!img_xy && z >= 2 && z < a.nk - 2 && full_vec) st16<T>(yrow_out, oy);
+            else store_images_vec<T, VX>(a.yout + ob, x, y, z, oy, a, true);
+            if constexpr (OpTraits<OP>::writes_a) {
+                if (full_vec) st16<T>(arow_out, oa);
+                else put_vec<T, VX>(arow_out, x, a.ni, oa);
+            }
         }
+        yrow_out += a.plane;
+        if constexpr (OpTraits<OP>::writes_a) arow_out += a.plane;
         cm2 = cm1; cm1 = c0; c0 = cp1; cp1 = cp2;
         if (__syncthreads_or(bad)) {
             if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
@@ -523,6 +577,17 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Tune& t, int* err) 
     a.lap_scale = (L.op == OP_EULER) ? c.s2 : c.s4;
     a.c_y = (T)L.c_y; a.c_acc = (T)L.c_acc;
     a.err = err;
+    {
+        // RHS4 as per-offset weights (used by the TMA RK stages; one nu per launch)
+        const double nl = L.nu * c.s4;
+        for (int d = 0; d < 3; ++d) {
+            a.w.m1[d] = (T)(8. * c.ca[d] + 16. * nl);
+            a.w.p1[d] = (T)(-8. * c.ca[d] + 16. * nl);
+            a.w.m2[d] = (T)(-c.ca[d] - nl);
+            a.w.p2[d] = (T)(c.ca[d] - nl);
+        }
+        a.w.c = (T)(-90. * nl);
+    }
     switch (L.op) {
         case OP_RK_S1: a.aout = (T*)L.acc; break;
         case OP_RK_S2:
@@ -601,6 +666,7 @@ cudaError_t set_attr_op() {
     return e;
 }
 
+
 // Ring depths per tile height: NS stencil slots (prefetch NS-3 planes ahead),
 // NP pointwise slots (prefetch NP-1 planes ahead).
 template <typename T, int OP>
@@ -616,10 +682,12 @@ cudaError_t launch_tma_op(const Geo& g, const StageLaunch& L, const KArgs<T>& a,
 template <typename T>
 cudaError_t launch_T(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err) {
     KArgs<T> a = make_args<T>(g, L, t, err);
+    // one diffusivity per item (batched slices with nufreq != 0): direct kernel
+    const bool tma = t.tma && !L.nu_items;
 #define SP_OPCASE(OPV)                                                              \
     case OPV:                                                                       \
-        return t.tma ? launch_tma_op<T, OPV>(g, L, a, t, s)                         \
-                     : launch_direct_T<T, OPV>(g, a, t, L.items, s);
+        return tma ? launch_tma_op<T, OPV>(g, L, a, t, s)                           \
+                   : launch_direct_T<T, OPV>(g, a, t, L.items, s);
     switch (L.op) {
         SP_OPCASE(OP_RK_S1)
         SP_OPCASE(OP_RK_S2)

@@ -110,12 +110,13 @@ struct sp_convection {
         auto it = tunes.find({prec, items});
         if (it != tunes.end()) return it->second;
         Tune t;
-        // default before tuning: TMA pipeline, 8-row tiles, z-chunks that give
-        // at least ~4 CTAs per SM
+        // default before tuning: TMA pipeline, 4-row tiles, z-chunks that give
+        // at least ~8 CTAs per SM
+        t.ty = 4;
         const int VX = prec == 0 ? 2 : 4;
-        const long long tiles = (long long)((P.ni + 32 * VX - 1) / (32 * VX)) * ((P.nj + 7) / 8) * items;
+        const long long tiles = (long long)((P.ni + 32 * VX - 1) / (32 * VX)) * ((P.nj + 3) / 4) * items;
         int zc = P.nk;
-        while (zc > 8 && tiles * ((P.nk + zc - 1) / zc) < 148LL * 4) zc = (zc + 1) / 2;
+        while (zc > 8 && tiles * ((P.nk + zc - 1) / zc) < 148LL * 8) zc = (zc + 1) / 2;
         t.zchunk = std::max(1, zc);
         return t;
     }
@@ -384,14 +385,15 @@ int sp_convection_synchronize(sp_convection* h) {
     return SP_OK;
 }
 
-int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int tma) {
+int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
     if (ty != 4 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "ty must be 4, 8 or 16");
     if (zchunk < 1) return fail(SP_ERR_INVALID, "zchunk must be >= 1");
+    if (kind < 0 || kind > 1) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct) or 1 (TMA)");
     Tune t;
     t.ty = ty;
     t.zchunk = zchunk;
-    t.tma = tma ? 1 : 0;
+    t.tma = kind;
     h->tunes[{precision, batch}] = t;
     for (auto& kv : h->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -536,12 +538,14 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     float best_ms = 1e30f;
     std::vector<int> zcs = {4, 8, 16, 32, 64};
     zcs.push_back(g.nk);
-    for (int tma = 1; tma >= 0; --tma)
+    // kernel kinds: 1 TMA pipeline, 0 direct loads
+    for (int kind = 1; kind >= 0; --kind)
         for (int ty : {4, 8, 16})
             for (int zc : zcs) {
                 if (zc > g.nk && zc != g.nk) continue;
                 Tune t;
-                t.tma = tma; t.ty = ty; t.zchunk = zc;
+                t.tma = kind;
+                t.ty = ty; t.zchunk = zc;
                 if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
                 cudaError_t e = launch_stage(g, L, t, s, h->err.as<int>());
                 if (e != cudaSuccess) { cudaGetLastError(); continue; }

@@ -10,8 +10,9 @@ TOL64 = 1e-12   # relative L2, FP64 kernels vs the oracle's restatement of the r
 TOL32 = 2e-5    # relative L2, FP32 kernels vs the oracle computing in FP32
 
 SIZES = [(32, 32, 32), (17, 19, 23), (16, 24, 40), (64, 8, 8), (2, 3, 5), (130, 66, 12)]
-SHAPES = [dict(tma=True, ty=8, zchunk=16), dict(tma=True, ty=4, zchunk=5), dict(tma=True, ty=16, zchunk=64),
-          dict(tma=False, ty=8, zchunk=7)]
+# kind: 0 direct loads, 1 TMA/mbarrier pipeline
+SHAPES = [dict(kind=1, ty=8, zchunk=16), dict(kind=1, ty=4, zchunk=5), dict(kind=1, ty=16, zchunk=64),
+          dict(kind=0, ty=8, zchunk=7), dict(kind=1, ty=4, zchunk=1), dict(kind=1, ty=8, zchunk=3)]
 
 
 def make(sp, n, **kw):
@@ -33,7 +34,7 @@ def orc_params(orc, n, args):
 def test_rk4_fp64_parity(sp, orc, n, shape):
     c, args = make(sp, n, cx=1.0, cy=-0.5, cz=0.25, nu0=0.02)
     s = SHAPES[shape]
-    c.set_tune(sp.SP_F64, 1, s["ty"], s["zchunk"], s["tma"])
+    c.set_tune(sp.SP_F64, 1, s["ty"], s["zchunk"], s["kind"])
     q0 = gaussian_noise(*n, seed=0)
     dt, steps = 1e-4, 7
     fin, fout = c.field(), c.field()
