@@ -37,7 +37,7 @@ class OrcParams(C.Structure):
 class OrcPararealCfg(C.Structure):
     _fields_ = [("endTime", C.c_double), ("timeSlices", C.c_int),
                 ("timeStepsFine", C.c_int), ("timeStepsCoarse", C.c_int),
-                ("kmax", C.c_int), ("async_", C.c_int), ("coarse", C.c_int)]
+                ("kmax", C.c_int), ("async_", C.c_int), ("coarse", C.c_int), ("coarse_delta", C.c_int)]
 
 
 def build() -> str:
@@ -165,9 +165,9 @@ def periodicity_jik(field):
 
 
 def parareal_cfg(endTime, timeSlices, timeStepsFine, timeStepsCoarse, kmax, async_=False,
-                 coarse=COARSE_EULER_F64) -> OrcPararealCfg:
+                 coarse=COARSE_EULER_F64, delta=False) -> OrcPararealCfg:
     return OrcPararealCfg(endTime, timeSlices, timeStepsFine, timeStepsCoarse, kmax,
-                          1 if async_ else 0, coarse)
+                          1 if async_ else 0, coarse, 1 if delta else 0)
 
 
 def parareal_derived(cfg):

@@ -52,6 +52,8 @@ typedef struct {
     int kmax;
     int async;             /* 1: split first fine step as in Parareal.h:119-124 */
     int coarse;            /* ORC_COARSE_* */
+    int coarse_delta;      /* 0: U = G(new) + F(old) - G(old) as Parareal.h:32-33;
+                              1: U = F(old) + G(new - old) (same value for this linear G) */
 } orc_parareal_cfg;
 
 /* Number of OpenMP threads used by the oracle (0 = OpenMP default). */
