@@ -147,6 +147,9 @@ typedef struct {
     int tol_kind;          /* SP_TOL_NONE: run kmax iterations, as the reference does */
     double tol;            /* stop once the chosen relative L2 quantity is below tol */
     int skip_converged;    /* 1: after iteration k, slices < k are exact; skip their fine runs */
+    int coarse_delta;      /* 0: U = G(new) + F(old) - G(old), the reference's UpdateStage
+                              (Parareal.h:32-33); 1: U = F(old) + G(new - old), equal for this
+                              linear G, with G applied to the FP64 increment (use with FP32 G) */
 } sp_parareal_cfg;
 
 typedef struct {

@@ -47,7 +47,7 @@ class SpPararealCfg(C.Structure):
     _fields_ = [("endTime", C.c_double), ("timeSlices", C.c_int), ("timeStepsFine", C.c_int),
                 ("timeStepsCoarse", C.c_int), ("kmax", C.c_int), ("async_", C.c_int),
                 ("coarse_scheme", C.c_int), ("coarse_precision", C.c_int), ("tol_kind", C.c_int),
-                ("tol", C.c_double), ("skip_converged", C.c_int)]
+                ("tol", C.c_double), ("skip_converged", C.c_int), ("coarse_delta", C.c_int)]
 
 
 class SpPararealReport(C.Structure):

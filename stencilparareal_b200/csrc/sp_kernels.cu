@@ -934,6 +934,68 @@ cudaError_t launch_update(const Geo& g64, const Geo& gc, const void* gnew, const
     return cudaGetLastError();
 }
 
+
+// Increment form of the correction (linear G): U_{r+1} = F_r + G(delta_r),
+// delta_{r+1} = U_{r+1}^new - U_{r+1}^old written, in coarse precision and with
+// its periodic images, as the next slice's coarse input; defect sums as k_update.
+template <typename TC>
+__global__ void k_update_delta(const TC* gd, const double* f, double* u, TC* dnext, double* def, Geo g, Geo gc,
+                               const int* item_lo, int item) {
+    if (item_lo && item < *item_lo) return;
+    const long long n = (long long)g.ni * g.nj * g.nk;
+    double s_d = 0., s_q = 0.;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % g.ni);
+        const int y = (int)((t / g.ni) % g.nj);
+        const int z = (int)(t / ((long long)g.ni * g.nj));
+        const long long o = g.origin + (long long)z * g.plane + (long long)y * g.px + x;
+        const long long oc = gc.origin + (long long)z * gc.plane + (long long)y * gc.px + x;
+        const double q = f[o] + (double)gd[oc];
+        const double d = q - u[o];
+        s_d += d * d;
+        s_q += q * q;
+        put_img<double>(u + g.origin, g, x, y, z, q);
+        put_img<TC>(dnext + gc.origin, gc, x, y, z, (TC)d);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s_d += __shfl_xor_sync(0xffffffffu, s_d, o);
+        s_q += __shfl_xor_sync(0xffffffffu, s_q, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(def, s_d);
+        atomicAdd(def + 1, s_q);
+    }
+}
+
+cudaError_t launch_update_delta(const Geo& g64, const Geo& gc, const void* gd, const double* f, double* u_next,
+                                void* d_next, double* def, const int* item_lo, int item, cudaStream_t s) {
+    add_launches(1);
+    const unsigned gr = grid_for((long long)g64.ni * g64.nj * g64.nk, 256);
+    if (gc.es == 8)
+        k_update_delta<double><<<gr, 256, 0, s>>>((const double*)gd, f, u_next, (double*)d_next, def, g64, gc,
+                                                  item_lo, item);
+    else
+        k_update_delta<float><<<gr, 256, 0, s>>>((const float*)gd, f, u_next, (float*)d_next, def, g64, gc, item_lo,
+                                                 item);
+    return cudaGetLastError();
+}
+
+// Zeroes field number *item_lo (if below nitems) of an array of fields of `bytes` each.
+__global__ void k_zero_item(unsigned char* base, long long bytes, int nitems, const int* item_lo) {
+    const int it = *item_lo;
+    if (it < 0 || it >= nitems) return;
+    ulonglong2* p = reinterpret_cast<ulonglong2*>(base + (long long)it * bytes);
+    const long long n = bytes / 16;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        p[t] = make_ulonglong2(0ull, 0ull);
+}
+
+cudaError_t launch_zero_item(void* base, long long bytes, int nitems, const int* item_lo, cudaStream_t s) {
+    add_launches(1);
+    k_zero_item<<<grid_for(bytes / 16, 256), 256, 0, s>>>(static_cast<unsigned char*>(base), bytes, nitems, item_lo);
+    return cudaGetLastError();
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
     // non-negative doubles order like their bit patterns
     atomicMax(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));

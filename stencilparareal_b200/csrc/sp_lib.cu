@@ -583,7 +583,8 @@ struct sp_parareal {
     DevBuf U;              // P+1 FP64 fields: slice inputs U_0..U_{P-1}, last slice result U_P
     DevBuf F;              // P FP64 fields: fine results
     DevBuf fs;             // 3P FP64 fields: fine scratch ya, yb, acc
-    DevBuf Gold;           // P coarse fields
+    DevBuf Gold;           // P coarse fields (reference form of the correction)
+    DevBuf D;              // P+1 coarse fields: slice increments (increment form)
     DevBuf Gt;             // 2 coarse fields (coarse result / ping-pong) + 3 coarse scratch
     DevBuf ctl;            // device control: item_lo (int) + defect sums (2P doubles) + err4
     DevBuf nutab;          // fine nu table (tsF x P) when nufreq != 0
@@ -603,6 +604,7 @@ struct sp_parareal {
     double* u(int r) const { return U.as<double>() + (size_t)r * g64.total; }
     double* f(int r) const { return F.as<double>() + (size_t)r * g64.total; }
     void* gold(int r) const { return static_cast<char*>(Gold.p) + (size_t)r * gc.total * gc.es; }
+    void* dlt(int r) const { return static_cast<char*>(D.p) + (size_t)r * gc.total * gc.es; }
     void* gt(int i) const { return static_cast<char*>(Gt.p) + (size_t)i * gc.total * gc.es; }
     int* itemlo() const { return static_cast<int*>(ctl.p); }
     double* def() const { return reinterpret_cast<double*>(static_cast<char*>(ctl.p) + 256); }
@@ -614,7 +616,8 @@ namespace {
 // Coarse propagation G of one field: src (FP64 slice input, geometry g64) ->
 // result in pr->gt(pr->coarse_res), n steps from t0.  Every kernel is gated by
 // item_lo against `item` when gate is set.
-int enqueue_coarse(sp_parareal* pr, const double* src, double t0, int n, bool gate, int item, cudaStream_t s) {
+int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0, int n, bool gate, int item,
+                   cudaStream_t s) {
     sp_convection* h = pr->prop;
     const int cp = pr->cprec;
     const Geo& gc = pr->gc;
@@ -627,7 +630,7 @@ int enqueue_coarse(sp_parareal* pr, const double* src, double t0, int n, bool ga
     void* yb = pr->gt(3);
     void* acc = pr->gt(4);
     // bring the input into coarse precision / geometry
-    SP_CUDA(launch_convert(gc, A, pr->g64, src, s, lo, item));
+    SP_CUDA(launch_convert(gc, A, gsrc, src, s, lo, item));
     void* cur = A;
     void* other = B;
     for (int i = 0; i < n; ++i) {
@@ -672,12 +675,23 @@ int build_iteration_graph(sp_parareal* pr) {
     }
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
     if (e == cudaSuccess) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
+    const bool delta = pr->cfg.coarse_delta != 0;
+    // increment form: the first slice still iterating receives an unchanged input
+    if (e == cudaSuccess && delta)
+        e = launch_zero_item(pr->D.p, (long long)pr->gc.total * pr->gc.es, P, pr->itemlo(), s);
     for (int r = 0; r < P && e == cudaSuccess && rc == SP_OK; ++r) {
         const double tStart = pr->slice * r;
-        rc = enqueue_coarse(pr, pr->u(r), tStart, pr->tsC, true, r, s);
-        if (rc) break;
-        e = launch_update(g, pr->gc, pr->gt(pr->coarse_res), pr->f(r), pr->gold(r), pr->u(r + 1), pr->def() + 2 * r,
-                          pr->itemlo(), r, s);
+        if (delta) {
+            rc = enqueue_coarse(pr, pr->dlt(r), pr->gc, tStart, pr->tsC, true, r, s);
+            if (rc) break;
+            e = launch_update_delta(g, pr->gc, pr->gt(pr->coarse_res), pr->f(r), pr->u(r + 1), pr->dlt(r + 1),
+                                    pr->def() + 2 * r, pr->itemlo(), r, s);
+        } else {
+            rc = enqueue_coarse(pr, pr->u(r), g, tStart, pr->tsC, true, r, s);
+            if (rc) break;
+            e = launch_update(g, pr->gc, pr->gt(pr->coarse_res), pr->f(r), pr->gold(r), pr->u(r + 1),
+                              pr->def() + 2 * r, pr->itemlo(), r, s);
+        }
     }
     if (e == cudaSuccess && rc == SP_OK) e = cudaEventRecordWithFlags(pr->ev[2], s, cudaEventRecordExternal);
     const long long nodes = launches() - before;
@@ -732,8 +746,10 @@ int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parar
     pr->gc = prop->g[pr->cprec];
     const size_t f64b = (size_t)pr->g64.total * 8;
     const size_t cb = (size_t)pr->gc.total * pr->gc.es;
+    const bool delta = c.coarse_delta != 0;
     if (pr->U.alloc((P + 1) * f64b) != cudaSuccess || pr->F.alloc(P * f64b) != cudaSuccess ||
-        pr->fs.alloc(3 * P * f64b) != cudaSuccess || pr->Gold.alloc(P * cb) != cudaSuccess ||
+        pr->fs.alloc(3 * P * f64b) != cudaSuccess ||
+        (delta ? pr->D.alloc((P + 1) * cb) : pr->Gold.alloc(P * cb)) != cudaSuccess ||
         pr->Gt.alloc(5 * cb) != cudaSuccess || pr->ctl.alloc(256 + (2 * P + 8) * sizeof(double)) != cudaSuccess)
         return fail(SP_ERR_NOMEM, "Parareal state for %d slices", P);
     if (prop->P.nufreq != 0.) {
@@ -801,22 +817,25 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
     // Predictor (Parareal.h:113-114).
     const size_t cb = (size_t)pr->gc.total * pr->gc.es;
+    const bool delta = pr->cfg.coarse_delta != 0;
     if (h->P.nufreq == 0.) {
         // With constant nu, U_r = G^{tsC*r}(q0) from t=0 equals the chain
         // U_{r+1} = G(U_r) step for step, and Gold_r = G(U_r) = U_{r+1}.
         for (int r = 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), pr->slice * r, pr->tsC, false, 0, s))) return rc;
-            SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if (!delta)
+                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
             SP_CUDA(launch_convert(g, pr->u(r + 1), pr->gc, pr->gt(pr->coarse_res), s));
         }
     } else {
         for (int r = 1; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(0), 0., pr->tsC * r, false, 0, s))) return rc;
+            if ((rc = enqueue_coarse(pr, pr->u(0), g, 0., pr->tsC * r, false, 0, s))) return rc;
             SP_CUDA(launch_convert(g, pr->u(r), pr->gc, pr->gt(pr->coarse_res), s));
         }
-        for (int r = 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), pr->slice * r, pr->tsC, false, 0, s))) return rc;
-            SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+        for (int r = delta ? P - 1 : 0; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if (!delta)
+                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
             if (r == P - 1) SP_CUDA(launch_convert(g, pr->u(P), pr->gc, pr->gt(pr->coarse_res), s));
         }
     }

@@ -86,12 +86,17 @@ class Parareal:
     tolerance ``tol`` on the relative L2 defect (``tol_kind='defect'``) or on
     the error against a given reference field (``tol_kind='reference'``), and
     ``skip_converged`` (slices < k are exact after k iterations; their fine
-    runs are skipped -- the results are bit-identical).
+    runs are skipped -- the results are bit-identical) and ``coarse_delta``:
+    the correction as U = F(old) + G(new - old) instead of the reference's
+    G(new) + F(old) - G(old) (equal for this linear G).  Applied to the FP64
+    increment, an FP32 G no longer leaves its rounding noise (~1e-7) in the
+    iterate; it is the default with ``coarse_precision='f32'``.
     """
 
     def __init__(self, propagator: Convection, initial: ConvectionField, solution: ConvectionField,
                  tStart: float, conf: RuntimeConfiguration, coarse: str = "euler", coarse_precision: str = "f64",
-                 tol: float = 0.0, tol_kind: str = "none", skip_converged: bool = True):
+                 tol: float = 0.0, tol_kind: str = "none", skip_converged: bool = True,
+                 coarse_delta: bool | None = None):
         self.prop = propagator
         self.initial = initial
         self.solution = solution
@@ -109,6 +114,9 @@ class Parareal:
         cfg.tol_kind = {"none": L.SP_TOL_NONE, "defect": L.SP_TOL_DEFECT, "reference": L.SP_TOL_REFERENCE}[tol_kind]
         cfg.tol = tol
         cfg.skip_converged = 1 if skip_converged else 0
+        if coarse_delta is None:  # increment form by default with an FP32 coarse propagator
+            coarse_delta = coarse_precision == "f32"
+        cfg.coarse_delta = 1 if coarse_delta else 0
         self.cfg = cfg
         h = C.c_void_p()
         L.check(L.lib().sp_parareal_create(propagator.handle, C.byref(cfg), C.byref(h)))
