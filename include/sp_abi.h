@@ -180,6 +180,20 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
 /* Parareal::DoSerial (Parareal.h:250-253): DoRK4(initial, solution, 0, dtF, tsF*P). */
 int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution);
 
+/* Many independent Parareal solves at once (grids, parameters, slice counts and
+ * step counts may all differ; all handles on one device).  Each instance's
+ * iteration (batched fine sweep + coarse sweep) is a child graph of one CUDA
+ * graph, launched once per iteration; converged instances are gated off on the
+ * device.  This replaces running the reference's MPI job once per instance.
+ * run: initial[i], solution[i] (and reference[i], may be NULL) are FP64 fields of
+ * instance i; reports[i] (may be NULL) as for sp_parareal_do_parallel; *seconds
+ * gets the device time of the whole run. */
+typedef struct sp_parareal_batch sp_parareal_batch;
+int sp_parareal_batch_create(sp_parareal* const* instances, int n, sp_parareal_batch** out);
+int sp_parareal_batch_destroy(sp_parareal_batch* b);
+int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* initial, double* const* solution,
+                          const double* const* reference, sp_parareal_report* reports, double* seconds);
+
 /* ---- adjoint ---------------------------------------------------------------- */
 /* Gradient of J = 0.5*||q_n - q_target||^2 through n FP64 RK4 steps (DoRK4
  * from tStart with step dt) with respect to q0, nu0 and (cx, cy, cz).

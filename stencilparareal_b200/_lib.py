@@ -98,6 +98,10 @@ _SIGS = {
     "sp_autotune": (_i, [_vp, _i, _i]),
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
     "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),
+    "sp_parareal_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
+    "sp_parareal_batch_destroy": (_i, [_vp]),
+    "sp_parareal_batch_run": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                                   C.POINTER(SpPararealReport), C.POINTER(_d)]),
 }
 
 

@@ -650,7 +650,7 @@ int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0,
 // Captures one Parareal iteration (Parareal.h:116-165 for every slice):
 //   F sweep   : tsF RK4 steps of all slices r >= item_lo, batched per stage
 //   G sweep   : for r = item_lo..P-1: G(U_r) (coarse), correction into U_{r+1}
-int build_iteration_graph(sp_parareal* pr) {
+int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long* nodes_out) {
     sp_convection* h = pr->prop;
     cudaStream_t s = h->stream();
     const int P = pr->P;
@@ -665,7 +665,7 @@ int build_iteration_graph(sp_parareal* pr) {
     SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     const long long before = launches();
     int rc = SP_OK;
-    cudaError_t e = cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal);
+    cudaError_t e = events ? cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal) : cudaSuccess;
     for (int i = 0; i < pr->tsF && e == cudaSuccess; ++i) {
         NuSrc nu;
         if (const_nu) nu.nu = h->P.nu0;
@@ -673,7 +673,7 @@ int build_iteration_graph(sp_parareal* pr) {
         const void* in = i == 0 ? (const void*)pr->u(0) : (const void*)pr->f(0);
         e = enqueue_rk4_step(g, 0, h->coef, pr->dtF, nu, in, pr->f(0), ya, yb, acc, P, pr->itemlo(), 0, tf, s, err);
     }
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
+    if (e == cudaSuccess && events) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
     if (e == cudaSuccess) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
     const bool delta = pr->cfg.coarse_delta != 0;
     // increment form: the first slice still iterating receives an unchanged input
@@ -693,7 +693,7 @@ int build_iteration_graph(sp_parareal* pr) {
                               pr->def() + 2 * r, pr->itemlo(), r, s);
         }
     }
-    if (e == cudaSuccess && rc == SP_OK) e = cudaEventRecordWithFlags(pr->ev[2], s, cudaEventRecordExternal);
+    if (e == cudaSuccess && rc == SP_OK && events) e = cudaEventRecordWithFlags(pr->ev[2], s, cudaEventRecordExternal);
     const long long nodes = launches() - before;
     add_launches(-nodes);
     cudaGraph_t graph = nullptr;
@@ -704,11 +704,58 @@ int build_iteration_graph(sp_parareal* pr) {
         return fail(SP_ERR_CUDA, "iteration capture: %s", cudaGetErrorString(e));
     }
     if (e2 != cudaSuccess) return fail(SP_ERR_CUDA, "iteration end capture: %s", cudaGetErrorString(e2));
-    e = cudaGraphInstantiate(&pr->iter, graph, 0);
+    *out = graph;
+    *nodes_out = nodes;
+    return SP_OK;
+}
+
+int build_iteration_graph(sp_parareal* pr) {
+    cudaGraph_t graph = nullptr;
+    long long nodes = 0;
+    int rc = capture_iteration(pr, true, &graph, &nodes);
+    if (rc) return rc;
+    cudaError_t e = cudaGraphInstantiate(&pr->iter, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, "iteration instantiate: %s", cudaGetErrorString(e));
     pr->iter_nodes = nodes;
     return SP_OK;
+}
+
+// The initial field into U_0 and the coarse predictor (Parareal.h:113-114):
+// U_r = G^{tsC*r}(q0) from t = 0, Gold_r = G(U_r) (reference form), and the
+// last slice's end value U_P = G(U_{P-1}), all enqueued on s.
+int enqueue_predictor(sp_parareal* pr, const double* initial, cudaStream_t s) {
+    sp_convection* h = pr->prop;
+    const int P = pr->P;
+    const Geo& g = pr->g64;
+    int rc = SP_OK;
+    // rank 0's qinitial is the initial field
+    SP_CUDA(cudaMemcpyAsync(pr->u(0), initial, g.total * 8, cudaMemcpyDeviceToDevice, s));
+    SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
+    const size_t cb = (size_t)pr->gc.total * pr->gc.es;
+    const bool delta = pr->cfg.coarse_delta != 0;
+    if (h->P.nufreq == 0.) {
+        // With constant nu, U_r = G^{tsC*r}(q0) from t=0 equals the chain
+        // U_{r+1} = G(U_r) step for step, and Gold_r = G(U_r) = U_{r+1}.
+        for (int r = 0; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if (!delta)
+                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+            SP_CUDA(launch_convert(g, pr->u(r + 1), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+    } else {
+        for (int r = 1; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(0), g, 0., pr->tsC * r, false, 0, s))) return rc;
+            SP_CUDA(launch_convert(g, pr->u(r), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+        for (int r = delta ? P - 1 : 0; r < P; ++r) {
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if (!delta)
+                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
+            if (r == P - 1) SP_CUDA(launch_convert(g, pr->u(P), pr->gc, pr->gt(pr->coarse_res), s));
+        }
+    }
+    return rc;
 }
 
 }  // namespace
@@ -812,33 +859,7 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     if (!pr->iter && (rc = build_iteration_graph(pr))) return rc;
 
     SP_CUDA(cudaEventRecord(pr->ev[3], s));
-    // rank 0's qinitial is the initial field
-    SP_CUDA(cudaMemcpyAsync(pr->u(0), initial, g.total * 8, cudaMemcpyDeviceToDevice, s));
-    SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
-    // Predictor (Parareal.h:113-114).
-    const size_t cb = (size_t)pr->gc.total * pr->gc.es;
-    const bool delta = pr->cfg.coarse_delta != 0;
-    if (h->P.nufreq == 0.) {
-        // With constant nu, U_r = G^{tsC*r}(q0) from t=0 equals the chain
-        // U_{r+1} = G(U_r) step for step, and Gold_r = G(U_r) = U_{r+1}.
-        for (int r = 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
-            if (!delta)
-                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
-            SP_CUDA(launch_convert(g, pr->u(r + 1), pr->gc, pr->gt(pr->coarse_res), s));
-        }
-    } else {
-        for (int r = 1; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(0), g, 0., pr->tsC * r, false, 0, s))) return rc;
-            SP_CUDA(launch_convert(g, pr->u(r), pr->gc, pr->gt(pr->coarse_res), s));
-        }
-        for (int r = delta ? P - 1 : 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
-            if (!delta)
-                SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
-            if (r == P - 1) SP_CUDA(launch_convert(g, pr->u(P), pr->gc, pr->gt(pr->coarse_res), s));
-        }
-    }
+    if ((rc = enqueue_predictor(pr, initial, s))) return rc;
     // Iterations (Parareal.h:116-165).
     int k = 0;
     double t_f = 0., t_c = 0.;
@@ -1020,5 +1041,178 @@ extern "C" int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* 
     if ((rc = sp_convection_synchronize(h))) return rc;
     if (grad_par) for (int i = 0; i < 4; ++i) grad_par[i] = hp[i];
     if (J) *J = lambda_n ? 0. : hp[4];
+    return SP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Many independent Parareal solves (uneven grids, parameters and slice
+// counts) advanced together: each instance's iteration graph becomes a child
+// graph of one parent graph, so one graph launch per iteration runs every
+// instance's batched fine sweep and coarse sweep concurrently.  An instance
+// that has converged (or used its kmax) gets item_lo = P, which turns its
+// kernels into immediate returns.
+struct sp_parareal_batch {
+    std::vector<sp_parareal*> ins;
+    int device = 0;
+    cudaStream_t root = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> done;
+    ~sp_parareal_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
+        if (root) cudaStreamDestroy(root);
+    }
+};
+
+extern "C" int sp_parareal_batch_create(sp_parareal* const* ins, int n, sp_parareal_batch** out) {
+    if (!ins || n < 1 || !out) return fail(SP_ERR_INVALID, "sp_parareal_batch_create: bad arguments");
+    *out = nullptr;
+    std::unique_ptr<sp_parareal_batch> b(new sp_parareal_batch());
+    for (int i = 0; i < n; ++i) {
+        if (!ins[i]) return fail(SP_ERR_INVALID, "null Parareal handle %d", i);
+        if (i && ins[i]->prop->device != ins[0]->prop->device)
+            return fail(SP_ERR_INVALID, "all instances must live on one device");
+        b->ins.push_back(ins[i]);
+    }
+    b->device = ins[0]->prop->device;
+    SP_CUDA(cudaSetDevice(b->device));
+    SP_CUDA(cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking));
+    for (auto& e : b->ev) SP_CUDA(cudaEventCreate(&e));
+    b->done.resize(n, nullptr);
+    for (auto& e : b->done) SP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaGraph_t parent = nullptr;
+    SP_CUDA(cudaGraphCreate(&parent, 0));
+    for (int i = 0; i < n; ++i) {
+        cudaGraph_t child = nullptr;
+        long long nodes = 0;
+        int rc = capture_iteration(b->ins[i], false, &child, &nodes);
+        if (rc) { cudaGraphDestroy(parent); return rc; }
+        cudaGraphNode_t node;
+        cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+        cudaGraphDestroy(child);
+        if (e != cudaSuccess) { cudaGraphDestroy(parent); return fail(SP_ERR_CUDA, "child graph: %s", cudaGetErrorString(e)); }
+        b->nodes += nodes;
+    }
+    cudaError_t e = cudaGraphInstantiate(&b->exec, parent, 0);
+    cudaGraphDestroy(parent);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
+    *out = b.release();
+    return SP_OK;
+}
+
+extern "C" int sp_parareal_batch_destroy(sp_parareal_batch* b) {
+    if (!b) return SP_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->root);
+    delete b;
+    return SP_OK;
+}
+
+extern "C" int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* initial, double* const* solution,
+                                     const double* const* reference, sp_parareal_report* reports,
+                                     double* seconds) {
+    if (!b || !initial || !solution) return fail(SP_ERR_INVALID, "sp_parareal_batch_run: null argument");
+    const int n = (int)b->ins.size();
+    SP_CUDA(cudaSetDevice(b->device));
+    cudaStream_t s = b->root;
+    for (int i = 0; i < n; ++i) {
+        sp_parareal* pr = b->ins[i];
+        if (!initial[i] || !solution[i]) return fail(SP_ERR_INVALID, "null field of instance %d", i);
+        int rc = pr->prop->ensure_scratch(pr->cprec, 1);
+        if (rc) return rc;
+        if (reports) {
+            std::memset(&reports[i], 0, sizeof reports[i]);
+            reports[i].tsFine = pr->tsF; reports[i].tsCoarse = pr->tsC;
+            reports[i].dtFine = pr->dtF; reports[i].dtCoarse = pr->dtC; reports[i].timeSliceSize = pr->slice;
+        }
+    }
+    SP_CUDA(cudaEventRecord(b->ev[0], s));
+    // predictors, one stream per instance handle, joined back into the root stream
+    for (int i = 0; i < n; ++i) {
+        sp_parareal* pr = b->ins[i];
+        cudaStream_t si = pr->prop->stream();
+        SP_CUDA(cudaStreamWaitEvent(si, b->ev[0], 0));
+        int rc = enqueue_predictor(pr, initial[i], si);
+        if (rc) return rc;
+        SP_CUDA(cudaEventRecord(b->done[i], si));
+        SP_CUDA(cudaStreamWaitEvent(s, b->done[i], 0));
+    }
+    std::vector<int> iters(n, 0);
+    std::vector<char> active(n, 1);
+    int kmax = 0;
+    for (auto* pr : b->ins) kmax = std::max(kmax, pr->cfg.kmax);
+    for (int k = 0; k < kmax; ++k) {
+        int n_active = 0;
+        for (int i = 0; i < n; ++i) {
+            sp_parareal* pr = b->ins[i];
+            if (active[i] && k >= pr->cfg.kmax) active[i] = 0;
+            *pr->h_itemlo = !active[i] ? pr->P : (pr->cfg.skip_converged ? std::min(k, pr->P) : 0);
+            n_active += active[i];
+            SP_CUDA(cudaMemcpyAsync(pr->itemlo(), pr->h_itemlo, sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+        if (!n_active) break;
+        SP_CUDA(cudaGraphLaunch(b->exec, s));
+        add_launches(b->nodes);
+        for (int i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            sp_parareal* pr = b->ins[i];
+            if (reference && reference[i]) {
+                SP_CUDA(cudaMemsetAsync(pr->err4(), 0, 4 * sizeof(double), s));
+                SP_CUDA(launch_errors(pr->g64, pr->u(pr->P), reference[i], pr->err4(), s));
+            }
+            SP_CUDA(cudaMemcpyAsync(pr->h_def, pr->def(), (2 * pr->P + 4) * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        SP_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            sp_parareal* pr = b->ins[i];
+            const int lo = pr->cfg.skip_converged ? std::min(k, pr->P) : 0;
+            double defect = 0.;
+            bool finite = true;
+            for (int r = lo; r < pr->P; ++r) {
+                const double num = pr->h_def[2 * r], den = pr->h_def[2 * r + 1];
+                if (!std::isfinite(num) || !std::isfinite(den)) finite = false;
+                if (den > 0) defect = std::max(defect, std::sqrt(num / den));
+            }
+            double el2 = 0., emax = 0.;
+            const bool has_ref = reference && reference[i];
+            if (has_ref) {
+                const double* e4 = pr->h_def + 2 * pr->P;
+                el2 = std::sqrt(e4[0] / e4[1]);
+                emax = e4[2] / e4[3];
+            }
+            iters[i] = k + 1;
+            if (reports) {
+                reports[i].defect[k] = defect;
+                reports[i].err_l2[k] = el2;
+                reports[i].err_max[k] = emax;
+                reports[i].fine_cell_updates +=
+                    (long long)(pr->P - lo) * pr->tsF * pr->g64.ni * pr->g64.nj * pr->g64.nk;
+            }
+            if (!finite) return fail(SP_ERR_NONFINITE, "instance %d: defect not finite at iteration %d", i, k + 1);
+            if ((pr->cfg.tol_kind == SP_TOL_DEFECT && defect < pr->cfg.tol) ||
+                (pr->cfg.tol_kind == SP_TOL_REFERENCE && has_ref && el2 < pr->cfg.tol) || k + 1 >= pr->P)
+                active[i] = 0;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        sp_parareal* pr = b->ins[i];
+        SP_CUDA(cudaMemcpyAsync(solution[i], pr->u(pr->P), pr->g64.total * 8, cudaMemcpyDeviceToDevice, s));
+        if (reports) reports[i].iterations = iters[i];
+    }
+    SP_CUDA(cudaEventRecord(b->ev[1], s));
+    SP_CUDA(cudaEventSynchronize(b->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+    if (seconds) *seconds = ms * 1e-3;
+    for (auto* pr : b->ins) {
+        int rc = sp_convection_synchronize(pr->prop);
+        if (rc) return rc;
+    }
     return SP_OK;
 }

@@ -167,3 +167,56 @@ def slice_bounds(P: int, world: int, rank: int):
 
 def cfl_ok(conf: RuntimeConfiguration) -> bool:
     return math.isfinite(conf.cflFine())
+
+
+def _report(rep) -> dict:
+    k = rep.iterations
+    return {"iterations": k, "tsFine": rep.tsFine, "tsCoarse": rep.tsCoarse, "dtFine": rep.dtFine,
+            "dtCoarse": rep.dtCoarse, "timeSliceSize": rep.timeSliceSize, "defect": list(rep.defect[:k]),
+            "err_l2": list(rep.err_l2[:k]), "err_max": list(rep.err_max[:k]),
+            "fine_cell_updates": rep.fine_cell_updates}
+
+
+class PararealBatch:
+    """Many independent Parareal solves advanced together on one GPU.
+
+    Each instance keeps its own grid, PDE parameters, slice count and step
+    counts; one CUDA graph launch per iteration runs all of them (the
+    instances' iteration graphs are child graphs of one parent graph) and an
+    instance stops once its tolerance is met, its kmax is used or it is exact
+    (k = P).
+    """
+
+    def __init__(self, instances):
+        self.instances = list(instances)
+        n = len(self.instances)
+        arr = (C.c_void_p * n)(*[p._h.value for p in self.instances])
+        h = C.c_void_p()
+        L.check(L.lib().sp_parareal_batch_create(arr, n, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            L.lib().sp_parareal_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, references=None):
+        """Runs every instance from its `initial` into its `solution`; returns (reports, seconds)."""
+        import torch
+        torch.cuda.synchronize()
+        n = len(self.instances)
+        ini = (C.c_void_p * n)(*[p.initial.ptr for p in self.instances])
+        sol = (C.c_void_p * n)(*[p.solution.ptr for p in self.instances])
+        ref = None
+        if references is not None:
+            ref = (C.c_void_p * n)(*[(r.ptr if r is not None else None) for r in references])
+        reps = (L.SpPararealReport * n)()
+        secs = C.c_double(0.0)
+        L.check(L.lib().sp_parareal_batch_run(self._h, ini, sol, ref, reps, C.byref(secs)))
+        return [_report(r) for r in reps], secs.value

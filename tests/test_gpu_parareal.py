@@ -152,3 +152,37 @@ def test_fp32_coarse_increment_form_removes_noise_floor(sp, orc):
         errs[delta] = par.DoParallel(reference=fref)["err_l2"]
     # state form: FP32 rounding of G(U) stalls the error; increment form keeps converging
     assert errs[True][-1] < 1e-3 * errs[False][-1], errs
+
+
+def test_batch_of_uneven_instances_equals_individual_runs(sp, orc):
+    from stencilparareal_b200.parareal import PararealBatch
+    specs = [  # n, nu0, c, P, coarse, precision
+        (12, 0.01, (1.0, -0.5, 0.3), 4, "rk4", "f32"),
+        (16, 0.003, (-0.7, 0.9, 0.1), 6, "rk4", "f32"),
+        (20, 0.05, (0.2, 0.2, -1.0), 3, "euler", "f64"),
+    ]
+    runs = []
+    for n, nu0, c, P, coarse, prec in specs:
+        conv = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, *c)
+        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, gridSize=n, endTime=0.01, timeStepsFine=100,
+                                       timeStepsCoarse=10, kmax=3)
+        q0 = gaussian_noise(n, seed=n)
+        fin, fa, fb, fref = conv.field(), conv.field(), conv.field(), conv.field()
+        conv.upload(fin, q0)
+        alone = sp.Parareal(conv, fin, fa, 0.0, conf, coarse=coarse, coarse_precision=prec)
+        alone.DoSerial()
+        fref.data.copy_(fa.data)
+        alone.DoParallel()
+        inb = sp.Parareal(conv, fin, fb, 0.0, conf, coarse=coarse, coarse_precision=prec)
+        runs.append((conv, alone, inb, fa, fb, fref, q0, (n, nu0, c, P, coarse, prec)))
+    batch = PararealBatch([r[2] for r in runs])
+    reps, secs = batch.run(references=[r[5] for r in runs])
+    assert secs > 0
+    for (conv, alone, inb, fa, fb, fref, q0, spec), rep in zip(runs, reps):
+        assert rep["iterations"] == 3
+        assert np.array_equal(conv.download(fa), conv.download(fb))
+        n, nu0, c, P, coarse, prec = spec
+        cfg = orc.parareal_cfg(0.01, P, 100, 10, 3, coarse=COARSE[(coarse, prec)], delta=(prec == "f32"))
+        qo, qs, em, el = orc.parareal(orc.params(n, nu0=nu0, cx=c[0], cy=c[1], cz=c[2]), cfg, q0)
+        assert rel_l2(conv.download(fb), qo) < (1e-11 if prec == "f64" else 1e-8)
+        assert abs(rep["err_l2"][-1] - el[-1]) <= 1e-3 * el[-1] + 1e-12
