@@ -33,6 +33,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -204,6 +206,90 @@ def parareal_summary(torch, sp, device):
             "fine_s": rep["seconds_fine"], "coarse_s": rep["seconds_coarse"]}
 
 
+def batch_summary(torch, sp, device, n_inst=48, seed=2):
+    """Config 4: 48 independent Parareal solves, grids drawn from {32,48,64,96}^3, nu log-uniform in
+    [1e-4, 1e-2], c uniform in [-1,1]^3, 8-24 slices; T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32
+    dt=1e-3 (totals rounded up to a multiple of the slice count), tolerance 1e-8 relative L2 against
+    each instance's serial FP64 fine solution."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import gaussian_noise
+    from stencilparareal_b200.parareal import PararealBatch
+    rng = np.random.default_rng(seed)
+    T = 0.05
+    specs = []
+    for i in range(n_inst):
+        n = int(rng.choice([32, 48, 64, 96]))
+        nu = float(10 ** rng.uniform(-4, -2))
+        c = rng.uniform(-1, 1, size=3)
+        P = int(rng.integers(8, 25))
+        specs.append((n, nu, tuple(float(v) for v in c), P))
+    tunes = {}
+    inst, refs, serial_s = [], [], 0.0
+    for i, (n, nu, c, P) in enumerate(specs):
+        conv = sp.Convection(n, n, n, 1.0 / n, nu, 0.0, *c, device=device)
+        if n not in tunes:
+            tunes[n] = (conv.autotune(sp.SP_F64, 16)["S2"], conv.autotune(sp.SP_F32, 1)["S2"])
+        t64, t32 = tunes[n]
+        conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
+        conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
+        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu, gridSize=n, endTime=T, timeStepsFine=5000,
+                                       timeStepsCoarse=50, kmax=P)
+        f0, fs, fr = conv.field(), conv.field(), conv.field()
+        conv.upload(f0, gaussian_noise(n, seed=seed + i))
+        par = sp.Parareal(conv, f0, fs, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
+                          tol_kind="reference")
+        t0 = time.perf_counter()
+        par.DoSerial()
+        conv.synchronize()
+        serial_s += time.perf_counter() - t0
+        fr.data.copy_(fs.data)
+        inst.append(par)
+        refs.append(fr)
+    batch = PararealBatch(inst)
+    reps, secs = batch.run(references=refs)   # warm (first launch)
+    reps, secs = batch.run(references=refs)
+    fine_cu = sum(r["fine_cell_updates"] for r in reps)
+    its = [r["iterations"] for r in reps]
+    errs = [r["err_l2"][-1] for r in reps]
+    return {"config": f"{n_inst} instances, grids {{32,48,64,96}}^3, nu log-uniform [1e-4,1e-2], c U[-1,1]^3, "
+                      "P 8-24, T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 dt=1e-3 (rounded per P), "
+                      "increment-form correction, stop at 1e-8 rel L2 vs serial fine; seed 2",
+            "instances": n_inst, "batch_s": secs, "serial_fine_sum_s": serial_s,
+            "speedup_vs_serial_sum": serial_s / secs if secs else None,
+            "iterations_max": max(its), "iterations_mean": sum(its) / len(its),
+            "err_l2_max": max(errs), "fine_gcups": fine_cu / secs / 1e9,
+            "grids": {str(k): sum(1 for s_ in specs if s_[0] == k) for k in (32, 48, 64, 96)},
+            "tunes": {str(k): v[0] for k, v in tunes.items()}}
+
+
+def adjoint_summary(torch, sp, device):
+    """Config 5: gradient of 0.5||q(T)-q_target||^2 through 400 RK4 FP64 steps at 128^3, checkpoint 20."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import gaussian_noise
+    from stencilparareal_b200.adjoint import misfit_gradient
+    n, steps, dt = 128, 400, 5e-5
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+    q0 = gaussian_noise(n, seed=0)
+    f0, ft, fp, fo = conv.field(), conv.field(), conv.field(), conv.field()
+    conv.upload(fp, q0 + 1e-2 * np.random.default_rng(3).uniform(-1, 1, size=q0.shape))
+    conv.DoRK4(fp, ft, 0.0, dt, steps)
+    conv.upload(f0, q0)
+    misfit_gradient(conv, f0, ft, 0.0, dt, steps, checkpoint_every=20)  # warm
+    conv.synchronize()
+    t0 = time.perf_counter()
+    J, g, gp = misfit_gradient(conv, f0, ft, 0.0, dt, steps, checkpoint_every=20)
+    t_adj = time.perf_counter() - t0
+    conv.DoRK4(f0, fo, 0.0, dt, steps)
+    conv.synchronize()
+    t0 = time.perf_counter()
+    conv.DoRK4(f0, fo, 0.0, dt, steps)
+    conv.synchronize()
+    t_fwd = time.perf_counter() - t0
+    return {"config": "128^3, 400 RK4 FP64 steps dt=5e-5, checkpoint every 20 steps, J=0.5||q(T)-q_target||^2",
+            "J": J, "grad_nu_c": gp, "gradient_s": t_adj, "forward_s": t_fwd,
+            "gradient_over_forward": t_adj / t_fwd}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -242,7 +328,7 @@ def main():
     else:
         ty, zc, kind = (int(x) for x in (args.tune if args.tune != "auto" else "4,8,1").split(","))
         conv.set_tune(sp.SP_F64, 1, ty, zc, kind)
-        tune = conv.tuned_config(sp.SP_F64, 1)
+        tune = conv.tuned_configs(sp.SP_F64, 1)
     q0 = fourier_ic(n)
     fin, fout = conv.field(), conv.field()
     conv.upload(fin, q0)
@@ -305,13 +391,15 @@ def main():
     e2e = cells * world / t_e2e / 1e9
 
     peak, peak_kind = peaks()
+    # the four stage kernels of an RK4 step are the whole timed region: per launch,
+    # 32 B x cells on average (128 B per cell-update) over the average launch time
     achieved = BYTES_PER_CELL_UPDATE * n ** 3 * STEPS_PER_RUN * args.steps / t_local / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                traffic = json.load(f).get("stage_kernel_bytes_per_cell_update")
+                traffic = json.load(f).get("bytes_per_launch_avg")
         except Exception:
             traffic = None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -321,16 +409,19 @@ def main():
                        "parallelism": f"replicas x{world}", "tune": tune},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+                         "traffic": traffic, "traffic_unit": "bytes per stage-kernel launch (ncu, profiles/)",
+                         "algorithmic_bytes_per_launch": BYTES_PER_CELL_UPDATE * n ** 3 / 4,
+                         "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8)},
             "gpu_launches": int(launches), "clocks": clk.summary()}
     if rank == 0 and world == 1:
         if not args.no_parareal:
-            try:
-                line["parareal"] = parareal_summary(torch, sp, device)
-            except Exception as ex:  # reported, not hidden
-                line["parareal"] = {"error": repr(ex)}
+            for key, fn in (("parareal", parareal_summary), ("batch", batch_summary), ("adjoint", adjoint_summary)):
+                try:
+                    line[key] = fn(torch, sp, device)
+                except Exception as ex:  # reported, not hidden
+                    line[key] = {"error": repr(ex)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:

@@ -230,13 +230,15 @@ const char* sp_last_error(void);
 int sp_abi_version(void);
 /* Kernel launches issued by this process so far (all handles). */
 long long sp_launch_count(void);
-/* Launch shape in use for a grid / batch: tile rows ty, z-chunk, kernel kind
- * (0 direct loads, 1 TMA/mbarrier pipeline). */
-int sp_tuned_config(sp_convection* h, int precision, int batch, int* ty, int* zchunk, int* kind);
-/* Runs the autotuner for this handle's grid at `batch` fields and precision. */
+/* Launch shape in use for a grid / batch and stage kernel `op` (0..3 = RK4 stages
+ * S1..S4, 4 = Euler): tile rows ty, z-chunk, kernel kind (0 direct loads, 1
+ * TMA/mbarrier pipeline). */
+int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* kind);
+/* Runs the autotuner for this handle's grid at `batch` fields and precision: every
+ * stage kernel gets the fastest of its candidate launch shapes. */
 int sp_autotune(sp_convection* h, int precision, int batch);
-/* Forces a launch shape for a precision and batch: ty in {4,8,16}, zchunk >= 1,
- * kind as in sp_tuned_config. */
+/* Forces one launch shape on every stage kernel for a precision and batch:
+ * ty in {4,8,16}, zchunk >= 1, kind as in sp_tuned_config. */
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind);
 
 #ifdef __cplusplus

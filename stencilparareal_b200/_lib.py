@@ -94,7 +94,7 @@ _SIGS = {
     "sp_last_error": (C.c_char_p, []),
     "sp_abi_version": (_i, []),
     "sp_launch_count": (_ll, []),
-    "sp_tuned_config": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "sp_tuned_config": (_i, [_vp, _i, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "sp_autotune": (_i, [_vp, _i, _i]),
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
     "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),

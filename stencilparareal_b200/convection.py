@@ -189,12 +189,17 @@ class Convection:
 
     def autotune(self, precision: int = L.SP_F64, batch: int = 1):
         self.call(L.lib().sp_autotune, self._h, precision, batch)
-        return self.tuned_config(precision, batch)
+        return self.tuned_configs(precision, batch)
 
-    def tuned_config(self, precision: int = L.SP_F64, batch: int = 1):
+    def tuned_config(self, precision: int = L.SP_F64, batch: int = 1, op: int = 1):
+        """Launch shape of stage kernel `op` (0..3 RK4 S1..S4, 4 Euler)."""
         ty, zc, tma = C.c_int(), C.c_int(), C.c_int()
-        L.check(L.lib().sp_tuned_config(self._h, precision, batch, C.byref(ty), C.byref(zc), C.byref(tma)))
+        L.check(L.lib().sp_tuned_config(self._h, precision, batch, op, C.byref(ty), C.byref(zc), C.byref(tma)))
         return {"ty": ty.value, "zchunk": zc.value, "kind": tma.value}
+
+    def tuned_configs(self, precision: int = L.SP_F64, batch: int = 1):
+        return {name: self.tuned_config(precision, batch, op)
+                for op, name in enumerate(("S1", "S2", "S3", "S4", "euler"))}
 
 
 def launch_count() -> int:

@@ -27,11 +27,20 @@ enum Op : int {
     OP_COUNT = 6
 };
 
-// Launch-shape choice for the stage kernels.
-struct Tune {
-    int ty = 8;       // rows of a CTA tile
-    int zchunk = 32;  // planes of one work item (a CTA's z-march)
+// Launch shape of one stage kernel.
+struct Shape {
+    int ty = 4;       // rows of a CTA tile
+    int zchunk = 8;   // planes marched by one CTA
     int tma = 1;      // 1: TMA/mbarrier pipeline kernel; 0: direct-load kernel
+};
+
+// Launch shapes of all stage kernels (indexed by Op, adjoint stages included).
+constexpr int kNumOps = OP_ADJ + 4;
+struct Tune {
+    Shape op[kNumOps];
+    void set_all(const Shape& s) {
+        for (auto& o : op) o = s;
+    }
 };
 
 // Coefficients of the right-hand side, precomputed on the host.

@@ -251,16 +251,24 @@ __device__ __forceinline__ T item_nl(const KArgs<T>& a, int b) {
     return (T)(nu * a.lap_scale);
 }
 
+// Reduces the four adjoint parameter sums over the CTA (warp shuffles, then
+// shared memory) and adds them to par_acc with one atomic per CTA and sum.
+// Every thread of the CTA must call it.
 __device__ __forceinline__ void reduce_par(double* g, double* par_acc, double gs_nu, double gs_c) {
-    // warp reduction, then one atomic per warp
+    __shared__ double red[32][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
         for (int o = 16; o > 0; o >>= 1) g[i] += __shfl_xor_sync(0xffffffffu, g[i], o);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(par_acc + 0, gs_nu * g[0]);
-        atomicAdd(par_acc + 1, gs_c * g[1]);
-        atomicAdd(par_acc + 2, gs_c * g[2]);
-        atomicAdd(par_acc + 3, gs_c * g[3]);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nwarp = (blockDim.x * blockDim.y + 31) / 32;
+    if ((tid & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) red[tid >> 5][i] = g[i];
+    __syncthreads();
+    if (tid < 4) {
+        double v = 0.;
+        for (int w = 0; w < nwarp; ++w) v += red[w][tid];
+        atomicAdd(par_acc + tid, (tid == 0 ? gs_nu : gs_c) * v);
     }
 }
 
@@ -559,7 +567,7 @@ bool make_tmap(CUtensorMap* tm, const Geo& g, const void* base, int items, int b
 }
 
 template <typename T>
-KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Tune& t, int* err) {
+KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err) {
     KArgs<T> a{};
     a.yout = (T*)L.yout;
     a.yin = (const T*)L.yin;
@@ -614,7 +622,7 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Tune& t, int* err) 
 }
 
 template <typename T, int OP>
-cudaError_t launch_direct_T(const Geo& g, const KArgs<T>& a, const Tune& t, int items, cudaStream_t s) {
+cudaError_t launch_direct_T(const Geo& g, const KArgs<T>& a, const Shape& t, int items, cudaStream_t s) {
     const int tyd = t.ty;
     dim3 grid((g.ni + 31) / 32, (g.nj + tyd - 1) / tyd, a.nzc * items);
     if (grid.z > 65535u) return cudaErrorInvalidConfiguration;
@@ -635,7 +643,7 @@ size_t tma_smem_bytes() {
 }
 
 template <typename T, int OP, int TY, int NS, int NP>
-cudaError_t launch_tma_T(const Geo& g, const StageLaunch& L, KArgs<T> a, const Tune& t, cudaStream_t s) {
+cudaError_t launch_tma_T(const Geo& g, const StageLaunch& L, KArgs<T> a, const Shape& t, cudaStream_t s) {
     constexpr int VX = V16<T>::N, TX = 32 * VX, W = TX + 2 * VX, H = TY + 4;
     CUtensorMap ts{}, t0{}, t1{}, t2{};
     if (!make_tmap(&ts, g, L.yin, L.items, W, H)) return cudaErrorInvalidValue;
@@ -670,7 +678,7 @@ cudaError_t set_attr_op() {
 // Ring depths per tile height: NS stencil slots (prefetch NS-3 planes ahead),
 // NP pointwise slots (prefetch NP-1 planes ahead).
 template <typename T, int OP>
-cudaError_t launch_tma_op(const Geo& g, const StageLaunch& L, const KArgs<T>& a, const Tune& t, cudaStream_t s) {
+cudaError_t launch_tma_op(const Geo& g, const StageLaunch& L, const KArgs<T>& a, const Shape& t, cudaStream_t s) {
     switch (t.ty) {
         case 4: return launch_tma_T<T, OP, 4, 6, 3>(g, L, a, t, s);
         case 8: return launch_tma_T<T, OP, 8, 5, 3>(g, L, a, t, s);
@@ -680,7 +688,7 @@ cudaError_t launch_tma_op(const Geo& g, const StageLaunch& L, const KArgs<T>& a,
 }
 
 template <typename T>
-cudaError_t launch_T(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err) {
+cudaError_t launch_T(const Geo& g, const StageLaunch& L, const Shape& t, cudaStream_t s, int* err) {
     KArgs<T> a = make_args<T>(g, L, t, err);
     // one diffusivity per item (batched slices with nufreq != 0): direct kernel
     const bool tma = t.tma && !L.nu_items;
@@ -727,8 +735,10 @@ cudaError_t prepare_kernels() {
 
 cudaError_t launch_stage(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err) {
     add_launches(1);
-    if (L.prec == 0) return launch_T<double>(g, L, t, s, err);
-    return launch_T<float>(g, L, t, s, err);
+    if (L.op < 0 || L.op >= kNumOps) return cudaErrorInvalidValue;
+    const Shape& sh = t.op[L.op];
+    if (L.prec == 0) return launch_T<double>(g, L, sh, s, err);
+    return launch_T<float>(g, L, sh, s, err);
 }
 
 // ---------------------------------------------------------------------------

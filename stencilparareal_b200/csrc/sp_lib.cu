@@ -98,6 +98,7 @@ struct sp_convection {
     DevBuf err;         // device error word
     DevBuf red;         // reduction scratch (8 doubles)
     DevBuf dense;       // staging for the host-buffer entry point
+    DevBuf adj_ckpt, adj_seg, adj_work, adj_par;  // adjoint workspace, kept between calls
     std::map<std::tuple<int, int>, Tune> tunes;  // (prec, items) -> tune
     std::map<std::tuple<int, const void*, double, double, int>, GraphEntry> graphs;
     cudaStream_t stream() const { return user ? user : own; }
@@ -109,15 +110,17 @@ struct sp_convection {
     Tune tune(int prec, int items) {
         auto it = tunes.find({prec, items});
         if (it != tunes.end()) return it->second;
-        Tune t;
         // default before tuning: TMA pipeline, 4-row tiles, z-chunks that give
-        // at least ~8 CTAs per SM
-        t.ty = 4;
+        // at least ~8 CTAs per SM, the same shape for every stage
+        Shape sh;
+        sh.ty = 4;
         const int VX = prec == 0 ? 2 : 4;
         const long long tiles = (long long)((P.ni + 32 * VX - 1) / (32 * VX)) * ((P.nj + 3) / 4) * items;
         int zc = P.nk;
         while (zc > 8 && tiles * ((P.nk + zc - 1) / zc) < 148LL * 8) zc = (zc + 1) / 2;
-        t.zchunk = std::max(1, zc);
+        sh.zchunk = std::max(1, zc);
+        Tune t;
+        t.set_all(sh);
         return t;
     }
     void drop_graphs() {
@@ -390,10 +393,12 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
     if (ty != 4 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "ty must be 4, 8 or 16");
     if (zchunk < 1) return fail(SP_ERR_INVALID, "zchunk must be >= 1");
     if (kind < 0 || kind > 1) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct) or 1 (TMA)");
+    Shape sh;
+    sh.ty = ty;
+    sh.zchunk = zchunk;
+    sh.tma = kind;
     Tune t;
-    t.ty = ty;
-    t.zchunk = zchunk;
-    t.tma = kind;
+    t.set_all(sh);
     h->tunes[{precision, batch}] = t;
     for (auto& kv : h->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -401,9 +406,9 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
     return SP_OK;
 }
 
-int sp_tuned_config(sp_convection* h, int precision, int batch, int* ty, int* zchunk, int* tma) {
+int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* tma) {
     if (!h) return fail(SP_ERR_INVALID, "null handle");
-    const Tune t = h->tune(precision, batch);
+    const Shape t = h->tune(precision, batch).op[op < 0 || op >= kNumOps ? OP_RK_S2 : op];
     if (ty) *ty = t.ty;
     if (zchunk) *zchunk = t.zchunk;
     if (tma) *tma = t.tma;
@@ -510,8 +515,9 @@ int sp_field_errors(sp_convection* h, const double* a, const double* b, double* 
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Autotuner: times the S2 stage (the most common kernel: one stencil input,
-// two pointwise inputs, two outputs) for each candidate launch shape.
+// Autotuner: for every stage kernel (RK4 S1..S4, Euler) times each candidate
+// launch shape (kernel kind x tile rows x z-chunk) on scratch fields and keeps
+// the fastest shape per stage.
 extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     int rc = check_handle(h);
     if (rc) return rc;
@@ -526,48 +532,48 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     cudaEvent_t e0, e1;
     SP_CUDA(cudaEventCreate(&e0));
     SP_CUDA(cudaEventCreate(&e1));
-    StageLaunch L;
-    L.op = OP_RK_S2;
-    L.prec = precision;
-    L.items = batch;
-    L.coef = h->coef;
-    L.nu = h->P.nu0;
-    L.yin = p; L.q = p + fb; L.acc = p + 2 * fb; L.yout = p + 3 * fb;
-    L.c_y = 1e-9; L.c_acc = 1e-9;
-    Tune best;
-    float best_ms = 1e30f;
+    Tune best = h->tune(precision, batch);
     std::vector<int> zcs = {4, 8, 16, 32, 64};
     zcs.push_back(g.nk);
-    // kernel kinds: 1 TMA pipeline, 0 direct loads
-    for (int kind = 1; kind >= 0; --kind)
-        for (int ty : {4, 8, 16})
-            for (int zc : zcs) {
-                if (zc > g.nk && zc != g.nk) continue;
-                Tune t;
-                t.tma = kind;
-                t.ty = ty; t.zchunk = zc;
-                if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
-                cudaError_t e = launch_stage(g, L, t, s, h->err.as<int>());
-                if (e != cudaSuccess) { cudaGetLastError(); continue; }
-                float ms = 1e30f;
-                for (int r = 0; r < 3; ++r) {
-                    cudaEventRecord(e0, s);
-                    launch_stage(g, L, t, s, h->err.as<int>());
-                    cudaEventRecord(e1, s);
-                    cudaEventSynchronize(e1);
-                    float m = 0;
-                    cudaEventElapsedTime(&m, e0, e1);
-                    ms = std::min(ms, m);
+    for (int op : {OP_RK_S1, OP_RK_S2, OP_RK_S3, OP_RK_S4, OP_EULER}) {
+        StageLaunch L;
+        L.op = op;
+        L.prec = precision;
+        L.items = batch;
+        L.coef = h->coef;
+        L.nu = h->P.nu0;
+        L.yin = p; L.q = p + fb; L.acc = p + 2 * fb; L.yout = p + 3 * fb;
+        L.c_y = 1e-9; L.c_acc = 1e-9;
+        float best_ms = 1e30f;
+        for (int kind = 1; kind >= 0; --kind)
+            for (int ty : {4, 8, 16})
+                for (int zc : zcs) {
+                    if (zc > g.nk && zc != g.nk) continue;
+                    if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
+                    Tune t;
+                    Shape sh;
+                    sh.tma = kind; sh.ty = ty; sh.zchunk = zc;
+                    t.set_all(sh);
+                    cudaError_t e = launch_stage(g, L, t, s, h->err.as<int>());
+                    if (e != cudaSuccess) { cudaGetLastError(); continue; }
+                    float ms = 1e30f;
+                    for (int r = 0; r < 3; ++r) {
+                        cudaEventRecord(e0, s);
+                        launch_stage(g, L, t, s, h->err.as<int>());
+                        cudaEventRecord(e1, s);
+                        cudaEventSynchronize(e1);
+                        float m = 0;
+                        cudaEventElapsedTime(&m, e0, e1);
+                        ms = std::min(ms, m);
+                    }
+                    if (ms < best_ms) { best_ms = ms; best.op[op] = sh; }
                 }
-                if (ms < best_ms) { best_ms = ms; best = t; }
-            }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     SP_CUDA(cudaStreamSynchronize(s));
     h->tunes[{precision, batch}] = best;
-    for (auto& kv : h->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    h->graphs.clear();
+    h->drop_graphs();
     return SP_OK;
 }
 
@@ -954,7 +960,10 @@ extern "C" int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* 
     const Geo& g = h->g[0];
     const size_t fb = (size_t)g.total * 8;
     if ((rc = h->ensure_scratch(0, 1))) return rc;
-    DevBuf ckpt, seg, work, par;
+    DevBuf& ckpt = h->adj_ckpt;
+    DevBuf& seg = h->adj_seg;
+    DevBuf& work = h->adj_work;
+    DevBuf& par = h->adj_par;
     // work: qn, lam, lam_acc, mu_a, mu_b, dummy
     if (ckpt.alloc(std::max(nseg, 1) * fb) != cudaSuccess || seg.alloc((size_t)4 * ck * fb) != cudaSuccess ||
         work.alloc(6 * fb) != cudaSuccess || par.alloc(8 * sizeof(double)) != cudaSuccess)

@@ -99,10 +99,12 @@ extern "C" int sp_do_rk4_noalloc(const sp_params* p, const double* in, double* o
     const Coef coef = make_coef(p->dx, p->cx, p->cy, p->cz, p->upwind);
     Tune t;
     {
-        const long long tiles = (long long)((p->ni + 63) / 64) * ((p->nj + 7) / 8);
+        Shape sh;
+        const long long tiles = (long long)((p->ni + 63) / 64) * ((p->nj + 3) / 4);
         int zc = p->nk;
-        while (zc > 8 && tiles * ((p->nk + zc - 1) / zc) < 148LL * 4) zc = (zc + 1) / 2;
-        t.zchunk = zc < 1 ? 1 : zc;
+        while (zc > 8 && tiles * ((p->nk + zc - 1) / zc) < 148LL * 8) zc = (zc + 1) / 2;
+        sh.zchunk = zc < 1 ? 1 : zc;
+        t.set_all(sh);
     }
     if ((e = cudaMemsetAsync(ds->err, 0, sizeof(int), s)) != cudaSuccess ||
         (e = launch_periodicity(g, const_cast<double*>(in), 1, s)) != cudaSuccess)
