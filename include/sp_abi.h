@@ -150,6 +150,8 @@ typedef struct {
     int coarse_delta;      /* 0: U = G(new) + F(old) - G(old), the reference's UpdateStage
                               (Parareal.h:32-33); 1: U = F(old) + G(new - old), equal for this
                               linear G, with G applied to the FP64 increment (use with FP32 G) */
+    int first_slice;       /* slice window of this handle: slices [first_slice, first_slice + */
+    int slice_count;       /* slice_count) of the timeSlices; 0 = all (one GPU runs everything) */
 } sp_parareal_cfg;
 
 typedef struct {
@@ -193,6 +195,18 @@ int sp_parareal_batch_create(sp_parareal* const* instances, int n, sp_parareal_b
 int sp_parareal_batch_destroy(sp_parareal_batch* b);
 int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* initial, double* const* solution,
                           const double* const* reference, sp_parareal_report* reports, double* seconds);
+
+/* Slice-window steps for a Parareal spread over several GPUs (the reference's
+ * one-rank-per-slice MPI ring, Parareal.h:110-171, with one rank per slice
+ * window).  Per iteration k each window runs window_fine, then -- after the
+ * previous window's window_coarse -- window_coarse with that window's last
+ * slice result as `u_first_new` (NULL for the window holding slice 0), and
+ * passes its own `q_last` on.  window_begin computes the window's predictor
+ * (from t = 0, as every reference rank does).  `defect` (may be NULL) gets
+ * the window's max relative L2 change of its slice results (synchronises). */
+int sp_parareal_window_begin(sp_parareal* pr, const double* initial);
+int sp_parareal_window_fine(sp_parareal* pr, int k);
+int sp_parareal_window_coarse(sp_parareal* pr, int k, const double* u_first_new, double* q_last, double* defect);
 
 /* ---- adjoint ---------------------------------------------------------------- */
 /* Gradient of J = 0.5*||q_n - q_target||^2 through n FP64 RK4 steps (DoRK4

@@ -47,7 +47,8 @@ class SpPararealCfg(C.Structure):
     _fields_ = [("endTime", C.c_double), ("timeSlices", C.c_int), ("timeStepsFine", C.c_int),
                 ("timeStepsCoarse", C.c_int), ("kmax", C.c_int), ("async_", C.c_int),
                 ("coarse_scheme", C.c_int), ("coarse_precision", C.c_int), ("tol_kind", C.c_int),
-                ("tol", C.c_double), ("skip_converged", C.c_int), ("coarse_delta", C.c_int)]
+                ("tol", C.c_double), ("skip_converged", C.c_int), ("coarse_delta", C.c_int),
+                ("first_slice", C.c_int), ("slice_count", C.c_int)]
 
 
 class SpPararealReport(C.Structure):
@@ -98,6 +99,9 @@ _SIGS = {
     "sp_autotune": (_i, [_vp, _i, _i]),
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
     "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),
+    "sp_parareal_window_begin": (_i, [_vp, _vp]),
+    "sp_parareal_window_fine": (_i, [_vp, _i]),
+    "sp_parareal_window_coarse": (_i, [_vp, _i, _vp, _vp, C.POINTER(_d)]),
     "sp_parareal_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "sp_parareal_batch_destroy": (_i, [_vp]),
     "sp_parareal_batch_run": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),

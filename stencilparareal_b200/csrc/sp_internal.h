@@ -103,8 +103,10 @@ cudaError_t launch_update(const Geo& g64, const Geo& gc, const void* gnew, const
 // coarse precision (images); defect sums into def[0..1].
 cudaError_t launch_update_delta(const Geo& g64, const Geo& gc, const void* gd, const double* f, double* u_next,
                                 void* d_next, double* def, const int* item_lo, int item, cudaStream_t s);
-// Zeroes field *item_lo of an array of nitems fields of `bytes` bytes each (bytes % 16 == 0).
-cudaError_t launch_zero_item(void* base, long long bytes, int nitems, const int* item_lo, cudaStream_t s);
+// Zeroes field *item_lo of an array of nitems fields of `bytes` bytes each (bytes % 16 == 0),
+// unless *item_lo < min_item.
+cudaError_t launch_zero_item(void* base, long long bytes, int nitems, const int* item_lo, cudaStream_t s,
+                             int min_item = 0);
 // err[0] += sum (a-b)^2 ; err[1] += sum b^2 ; err[2] = max |a-b| ; err[3] = max |a|   (FP64 fields)
 cudaError_t launch_errors(const Geo& g, const double* a, const double* b, double* acc4, cudaStream_t s);
 // Pointwise axpby on FP64 fields (interior+images): out = alpha*x + beta*y (y may be null).

@@ -990,19 +990,21 @@ cudaError_t launch_update_delta(const Geo& g64, const Geo& gc, const void* gd, c
     return cudaGetLastError();
 }
 
-// Zeroes field number *item_lo (if below nitems) of an array of fields of `bytes` each.
-__global__ void k_zero_item(unsigned char* base, long long bytes, int nitems, const int* item_lo) {
+// Zeroes field number *item_lo (if in [min_item, nitems)) of an array of fields of `bytes` each.
+__global__ void k_zero_item(unsigned char* base, long long bytes, int nitems, const int* item_lo, int min_item) {
     const int it = *item_lo;
-    if (it < 0 || it >= nitems) return;
+    if (it < min_item || it >= nitems) return;
     ulonglong2* p = reinterpret_cast<ulonglong2*>(base + (long long)it * bytes);
     const long long n = bytes / 16;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         p[t] = make_ulonglong2(0ull, 0ull);
 }
 
-cudaError_t launch_zero_item(void* base, long long bytes, int nitems, const int* item_lo, cudaStream_t s) {
+cudaError_t launch_zero_item(void* base, long long bytes, int nitems, const int* item_lo, cudaStream_t s,
+                             int min_item) {
     add_launches(1);
-    k_zero_item<<<grid_for(bytes / 16, 256), 256, 0, s>>>(static_cast<unsigned char*>(base), bytes, nitems, item_lo);
+    k_zero_item<<<grid_for(bytes / 16, 256), 256, 0, s>>>(static_cast<unsigned char*>(base), bytes, nitems, item_lo,
+                                                         min_item);
     return cudaGetLastError();
 }
 

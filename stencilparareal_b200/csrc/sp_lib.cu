@@ -56,13 +56,18 @@ struct DevBuf {
         p = nullptr;
         bytes = 0;
     }
+    // Allocates and zeroes n bytes.  The zeroing is complete on return: the
+    // library's work runs on non-blocking streams, which do not order after
+    // cudaMemset's legacy-stream work.
     cudaError_t alloc(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
         release();
         cudaError_t e = cudaMalloc(&p, n);
         if (e != cudaSuccess) { p = nullptr; return e; }
         bytes = n;
-        return cudaMemset(p, 0, n);
+        e = cudaMemset(p, 0, n);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        return e;
     }
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
@@ -382,7 +387,8 @@ int sp_convection_synchronize(sp_convection* h) {
     int word = 0;
     SP_CUDA(cudaMemcpy(&word, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (word != 0) {
-        cudaMemset(h->err.p, 0, sizeof(int));
+        cudaMemsetAsync(h->err.p, 0, sizeof(int), h->stream());
+        cudaStreamSynchronize(h->stream());
         return fail(SP_ERR_TIMEOUT, "a bounded in-kernel wait gave up (device error word %d)", word);
     }
     return SP_OK;
@@ -583,6 +589,10 @@ struct sp_parareal {
     sp_convection* prop = nullptr;
     sp_parareal_cfg cfg{};
     int P = 0, tsF = 0, tsC = 0;
+    int first = 0, Pglobal = 0;  // slice window [first, first + P) of Pglobal slices
+    cudaGraphExec_t wfine = nullptr, wcoarse = nullptr;  // window-mode graphs
+    long long wfine_nodes = 0, wcoarse_nodes = 0;
+    DevBuf Z;              // one zero coarse field (window-mode injection)
     double dtF = 0, dtC = 0, slice = 0;
     int cprec = 0;         // coarse precision index
     Geo g64, gc;
@@ -602,6 +612,8 @@ struct sp_parareal {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     ~sp_parareal() {
         if (iter) cudaGraphExecDestroy(iter);
+        if (wfine) cudaGraphExecDestroy(wfine);
+        if (wcoarse) cudaGraphExecDestroy(wcoarse);
         if (h_itemlo) cudaFreeHost(h_itemlo);
         if (h_def) cudaFreeHost(h_def);
         for (auto& e : ev)
@@ -656,7 +668,11 @@ int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0,
 // Captures one Parareal iteration (Parareal.h:116-165 for every slice):
 //   F sweep   : tsF RK4 steps of all slices r >= item_lo, batched per stage
 //   G sweep   : for r = item_lo..P-1: G(U_r) (coarse), correction into U_{r+1}
-int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long* nodes_out) {
+// parts: 1 = F sweep, 2 = G sweep, 3 = both.  zero_min: in the increment form the
+// G sweep zeroes the increment of its first iterating slice unless that is a slice
+// below zero_min (a window's slice 0 gets its increment from the previous window).
+int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long* nodes_out, int parts = 3,
+                      int zero_min = 0) {
     sp_convection* h = pr->prop;
     cudaStream_t s = h->stream();
     const int P = pr->P;
@@ -672,7 +688,7 @@ int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long*
     const long long before = launches();
     int rc = SP_OK;
     cudaError_t e = events ? cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal) : cudaSuccess;
-    for (int i = 0; i < pr->tsF && e == cudaSuccess; ++i) {
+    for (int i = 0; i < pr->tsF && e == cudaSuccess && (parts & 1); ++i) {
         NuSrc nu;
         if (const_nu) nu.nu = h->P.nu0;
         else nu.items = pr->nutab.as<double>() + (size_t)i * P;
@@ -680,13 +696,13 @@ int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long*
         e = enqueue_rk4_step(g, 0, h->coef, pr->dtF, nu, in, pr->f(0), ya, yb, acc, P, pr->itemlo(), 0, tf, s, err);
     }
     if (e == cudaSuccess && events) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
-    if (e == cudaSuccess) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
+    if (e == cudaSuccess && (parts & 2)) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
     const bool delta = pr->cfg.coarse_delta != 0;
     // increment form: the first slice still iterating receives an unchanged input
-    if (e == cudaSuccess && delta)
-        e = launch_zero_item(pr->D.p, (long long)pr->gc.total * pr->gc.es, P, pr->itemlo(), s);
-    for (int r = 0; r < P && e == cudaSuccess && rc == SP_OK; ++r) {
-        const double tStart = pr->slice * r;
+    if (e == cudaSuccess && delta && (parts & 2))
+        e = launch_zero_item(pr->D.p, (long long)pr->gc.total * pr->gc.es, P, pr->itemlo(), s, zero_min);
+    for (int r = 0; r < P && e == cudaSuccess && rc == SP_OK && (parts & 2); ++r) {
+        const double tStart = pr->slice * (pr->first + r);
         if (delta) {
             rc = enqueue_coarse(pr, pr->dlt(r), pr->gc, tStart, pr->tsC, true, r, s);
             if (rc) break;
@@ -740,22 +756,28 @@ int enqueue_predictor(sp_parareal* pr, const double* initial, cudaStream_t s) {
     SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
     const size_t cb = (size_t)pr->gc.total * pr->gc.es;
     const bool delta = pr->cfg.coarse_delta != 0;
+    const int F0 = pr->first;
+    if (F0 > 0) {
+        // a window's first slice: G^{tsC*first}(q0) from t = 0, as the reference's rank `first` computes it
+        if ((rc = enqueue_coarse(pr, initial, g, 0., pr->tsC * F0, false, 0, s))) return rc;
+        SP_CUDA(launch_convert(g, pr->u(0), pr->gc, pr->gt(pr->coarse_res), s));
+    }
     if (h->P.nufreq == 0.) {
         // With constant nu, U_r = G^{tsC*r}(q0) from t=0 equals the chain
         // U_{r+1} = G(U_r) step for step, and Gold_r = G(U_r) = U_{r+1}.
         for (int r = 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * (F0 + r), pr->tsC, false, 0, s))) return rc;
             if (!delta)
                 SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
             SP_CUDA(launch_convert(g, pr->u(r + 1), pr->gc, pr->gt(pr->coarse_res), s));
         }
     } else {
         for (int r = 1; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(0), g, 0., pr->tsC * r, false, 0, s))) return rc;
+            if ((rc = enqueue_coarse(pr, initial, g, 0., pr->tsC * (F0 + r), false, 0, s))) return rc;
             SP_CUDA(launch_convert(g, pr->u(r), pr->gc, pr->gt(pr->coarse_res), s));
         }
         for (int r = delta ? P - 1 : 0; r < P; ++r) {
-            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * r, pr->tsC, false, 0, s))) return rc;
+            if ((rc = enqueue_coarse(pr, pr->u(r), g, pr->slice * (F0 + r), pr->tsC, false, 0, s))) return rc;
             if (!delta)
                 SP_CUDA(cudaMemcpyAsync(pr->gold(r), pr->gt(pr->coarse_res), cb, cudaMemcpyDeviceToDevice, s));
             if (r == P - 1) SP_CUDA(launch_convert(g, pr->u(P), pr->gc, pr->gt(pr->coarse_res), s));
@@ -783,17 +805,23 @@ int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parar
     std::unique_ptr<sp_parareal> pr(new sp_parareal());
     pr->prop = prop;
     pr->cfg = c;
-    const int P = c.timeSlices;
+    const int PG = c.timeSlices;
+    if (c.first_slice < 0 || c.slice_count < 0 || c.first_slice + std::max(c.slice_count, 1) > PG ||
+        (c.slice_count == 0 && c.first_slice != 0))
+        return fail(SP_ERR_INVALID, "slice window [%d, +%d) outside %d slices", c.first_slice, c.slice_count, PG);
+    const int P = c.slice_count > 0 ? c.slice_count : PG;
     pr->P = P;
-    // RuntimeConfiguration.cpp:133-151: totals rounded up to a multiple of P.
+    pr->first = c.first_slice;
+    pr->Pglobal = PG;
+    // RuntimeConfiguration.cpp:133-151: totals rounded up to a multiple of the slice count.
     int f = c.timeStepsFine, g = c.timeStepsCoarse;
-    if (f % P != 0) f = (f / P + 1) * P;
-    if (g % P != 0) g = (g / P + 1) * P;
-    pr->tsF = f / P;
-    pr->tsC = g / P;
+    if (f % PG != 0) f = (f / PG + 1) * PG;
+    if (g % PG != 0) g = (g / PG + 1) * PG;
+    pr->tsF = f / PG;
+    pr->tsC = g / PG;
     pr->dtF = c.endTime / f;  // RuntimeConfiguration.h:54-65
     pr->dtC = c.endTime / g;
-    pr->slice = c.endTime / P;
+    pr->slice = c.endTime / PG;
     pr->cprec = c.coarse_precision == SP_F64 ? 0 : 1;
     pr->g64 = prop->g[0];
     pr->gc = prop->g[pr->cprec];
@@ -802,7 +830,7 @@ int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parar
     const bool delta = c.coarse_delta != 0;
     if (pr->U.alloc((P + 1) * f64b) != cudaSuccess || pr->F.alloc(P * f64b) != cudaSuccess ||
         pr->fs.alloc(3 * P * f64b) != cudaSuccess ||
-        (delta ? pr->D.alloc((P + 1) * cb) : pr->Gold.alloc(P * cb)) != cudaSuccess ||
+        (delta ? pr->D.alloc((P + 1) * cb) : pr->Gold.alloc(P * cb)) != cudaSuccess || pr->Z.alloc(cb) != cudaSuccess ||
         pr->Gt.alloc(5 * cb) != cudaSuccess || pr->ctl.alloc(256 + (2 * P + 8) * sizeof(double)) != cudaSuccess)
         return fail(SP_ERR_NOMEM, "Parareal state for %d slices", P);
     if (prop->P.nufreq != 0.) {
@@ -811,11 +839,12 @@ int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parar
         // step of the asynchronous variant (Parareal.h:119-124).
         std::vector<double> tab((size_t)pr->tsF * P);
         for (int r = 0; r < P; ++r) {
-            const double tStart = pr->slice * r;
+            const double tStart = pr->slice * (pr->first + r);
             const double tStartFine = tStart + pr->dtF;
             for (int i = 0; i < pr->tsF; ++i) {
                 double t;
-                if (c.async && r != 0) t = i == 0 ? tStart : (i == 1 ? tStartFine : tStartFine + (i - 1) * pr->dtF);
+                if (c.async && pr->first + r != 0)
+                    t = i == 0 ? tStart : (i == 1 ? tStartFine : tStartFine + (i - 1) * pr->dtF);
                 else t = i == 0 ? tStart : tStart + i * pr->dtF;
                 tab[(size_t)i * P + r] = computenu(prop->P.nu0, prop->P.nufreq, t);
             }
@@ -841,7 +870,7 @@ int sp_parareal_destroy(sp_parareal* pr) {
 int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution) {
     if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
     // Parareal::DoSerial (Parareal.h:250-253)
-    return sp_do_rk4(pr->prop, initial, solution, 0., pr->dtF, pr->tsF * pr->P);
+    return sp_do_rk4(pr->prop, initial, solution, 0., pr->dtF, pr->tsF * pr->Pglobal);
 }
 
 int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solution, const double* reference,
@@ -851,6 +880,7 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     int rc = check_handle(h);
     if (rc) return rc;
     if (!initial || !solution) return fail(SP_ERR_INVALID, "null field");
+    if (pr->P != pr->Pglobal) return fail(SP_ERR_STATE, "a slice-window handle runs through sp_parareal_window_*");
     cudaStream_t s = h->stream();
     if (capturing(s)) return fail(SP_ERR_STATE, "DoParallel cannot run inside a stream capture");
     const int P = pr->P;
@@ -1084,6 +1114,7 @@ extern "C" int sp_parareal_batch_create(sp_parareal* const* ins, int n, sp_parar
     std::unique_ptr<sp_parareal_batch> b(new sp_parareal_batch());
     for (int i = 0; i < n; ++i) {
         if (!ins[i]) return fail(SP_ERR_INVALID, "null Parareal handle %d", i);
+        if (ins[i]->P != ins[i]->Pglobal) return fail(SP_ERR_INVALID, "instance %d is a slice window", i);
         if (i && ins[i]->prop->device != ins[0]->prop->device)
             return fail(SP_ERR_INVALID, "all instances must live on one device");
         b->ins.push_back(ins[i]);
@@ -1222,6 +1253,96 @@ extern "C" int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* 
     for (auto* pr : b->ins) {
         int rc = sp_convection_synchronize(pr->prop);
         if (rc) return rc;
+    }
+    return SP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Slice-window steps (Parareal over several GPUs; the exchange between windows
+// is the caller's, e.g. NCCL send/recv of the boundary field).
+namespace {
+int window_graphs(sp_parareal* pr) {
+    if (pr->wfine) return SP_OK;
+    cudaGraph_t g1 = nullptr, g2 = nullptr;
+    long long n1 = 0, n2 = 0;
+    int rc = capture_iteration(pr, false, &g1, &n1, 1, 0);
+    if (rc) return rc;
+    rc = capture_iteration(pr, false, &g2, &n2, 2, 1);
+    if (rc) { cudaGraphDestroy(g1); return rc; }
+    cudaError_t e = cudaGraphInstantiate(&pr->wfine, g1, 0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&pr->wcoarse, g2, 0);
+    cudaGraphDestroy(g1);
+    cudaGraphDestroy(g2);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "window graphs: %s", cudaGetErrorString(e));
+    pr->wfine_nodes = n1;
+    pr->wcoarse_nodes = n2;
+    return SP_OK;
+}
+
+int window_itemlo(sp_parareal* pr, int k) {
+    // global slices < k are exact after k iterations; local index of the first that is not
+    return pr->cfg.skip_converged ? std::max(0, std::min(k - pr->first, pr->P)) : 0;
+}
+}  // namespace
+
+extern "C" int sp_parareal_window_begin(sp_parareal* pr, const double* initial) {
+    if (!pr || !initial) return fail(SP_ERR_INVALID, "null argument");
+    int rc = check_handle(pr->prop);
+    if (rc) return rc;
+    cudaStream_t s = pr->prop->stream();
+    if ((rc = pr->prop->ensure_scratch(pr->cprec, 1))) return rc;
+    if ((rc = window_graphs(pr))) return rc;
+    return enqueue_predictor(pr, initial, s);
+}
+
+extern "C" int sp_parareal_window_fine(sp_parareal* pr, int k) {
+    if (!pr || k < 0) return fail(SP_ERR_INVALID, "bad argument");
+    int rc = check_handle(pr->prop);
+    if (rc) return rc;
+    if ((rc = window_graphs(pr))) return rc;
+    cudaStream_t s = pr->prop->stream();
+    *pr->h_itemlo = window_itemlo(pr, k);
+    SP_CUDA(cudaMemcpyAsync(pr->itemlo(), pr->h_itemlo, sizeof(int), cudaMemcpyHostToDevice, s));
+    SP_CUDA(cudaGraphLaunch(pr->wfine, s));
+    add_launches(pr->wfine_nodes);
+    return SP_OK;
+}
+
+extern "C" int sp_parareal_window_coarse(sp_parareal* pr, int k, const double* u_first_new, double* q_last,
+                                         double* defect) {
+    if (!pr || k < 0) return fail(SP_ERR_INVALID, "bad argument");
+    int rc = check_handle(pr->prop);
+    if (rc) return rc;
+    if ((rc = window_graphs(pr))) return rc;
+    if ((pr->first > 0) != (u_first_new != nullptr))
+        return fail(SP_ERR_INVALID, "u_first_new is required exactly when the window does not start at slice 0");
+    cudaStream_t s = pr->prop->stream();
+    const Geo& g = pr->g64;
+    const int lo = window_itemlo(pr, k);
+    // the window's first slice input: U_0 <- received value (the reference's
+    // MPI_Recv into qinitial, Parareal.h:132-139); increment form: D_0 = new - old
+    if (pr->cfg.coarse_delta) {
+        if (u_first_new) {
+            SP_CUDA(launch_update_delta(g, pr->gc, pr->Z.p, u_first_new, pr->u(0), pr->dlt(0), pr->err4(), nullptr,
+                                        0, s));
+        } else {
+            SP_CUDA(cudaMemsetAsync(pr->dlt(0), 0, (size_t)pr->gc.total * pr->gc.es, s));
+        }
+    } else if (u_first_new) {
+        SP_CUDA(cudaMemcpyAsync(pr->u(0), u_first_new, g.total * 8, cudaMemcpyDeviceToDevice, s));
+        SP_CUDA(launch_periodicity(g, pr->u(0), 1, s));
+    }
+    (void)lo;
+    SP_CUDA(cudaGraphLaunch(pr->wcoarse, s));
+    add_launches(pr->wcoarse_nodes);
+    if (q_last) SP_CUDA(cudaMemcpyAsync(q_last, pr->u(pr->P), g.total * 8, cudaMemcpyDeviceToDevice, s));
+    if (defect) {
+        SP_CUDA(cudaMemcpyAsync(pr->h_def, pr->def(), 2 * pr->P * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SP_CUDA(cudaStreamSynchronize(s));
+        double d = 0.;
+        for (int r = window_itemlo(pr, k); r < pr->P; ++r)
+            if (pr->h_def[2 * r + 1] > 0) d = std::max(d, std::sqrt(pr->h_def[2 * r] / pr->h_def[2 * r + 1]));
+        *defect = d;
     }
     return SP_OK;
 }

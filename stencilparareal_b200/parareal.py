@@ -96,7 +96,7 @@ class Parareal:
     def __init__(self, propagator: Convection, initial: ConvectionField, solution: ConvectionField,
                  tStart: float, conf: RuntimeConfiguration, coarse: str = "euler", coarse_precision: str = "f64",
                  tol: float = 0.0, tol_kind: str = "none", skip_converged: bool = True,
-                 coarse_delta: bool | None = None):
+                 coarse_delta: bool | None = None, first_slice: int = 0, slice_count: int = 0):
         self.prop = propagator
         self.initial = initial
         self.solution = solution
@@ -117,6 +117,8 @@ class Parareal:
         if coarse_delta is None:  # increment form by default with an FP32 coarse propagator
             coarse_delta = coarse_precision == "f32"
         cfg.coarse_delta = 1 if coarse_delta else 0
+        cfg.first_slice = int(first_slice)
+        cfg.slice_count = int(slice_count)
         self.cfg = cfg
         h = C.c_void_p()
         L.check(L.lib().sp_parareal_create(propagator.handle, C.byref(cfg), C.byref(h)))
@@ -220,3 +222,91 @@ class PararealBatch:
         secs = C.c_double(0.0)
         L.check(L.lib().sp_parareal_batch_run(self._h, ini, sol, ref, reps, C.byref(secs)))
         return [_report(r) for r in reps], secs.value
+
+
+class WindowParareal(Parareal):
+    """Slices [first, first+count) of a Parareal whose other slices live on other GPUs.
+
+    The steps of one iteration follow one rank of the reference's ring
+    (Parareal.h:116-165): fine(k) runs the window's batched fine sweep;
+    coarse(k, u_first_new) takes the previous window's last slice result
+    (the reference's MPI_Recv into qinitial), runs the coarse sweep and the
+    corrections, and leaves the window's last slice result in `boundary` for
+    the next window (the reference's MPI_Send).
+    """
+
+    def __init__(self, propagator, initial, solution, tStart, conf, first: int, count: int, **kw):
+        super().__init__(propagator, initial, solution, tStart, conf, first_slice=first, slice_count=count, **kw)
+        self.first, self.count = first, count
+        self.boundary = propagator.field(name="boundary")
+
+    def make_recv_buffer(self):
+        return self.prop.field(name="inbound")
+
+    def begin(self):
+        self.prop.call(L.lib().sp_parareal_window_begin, self._h, C.c_void_p(self.initial.ptr))
+
+    def fine(self, k: int):
+        self.prop.call(L.lib().sp_parareal_window_fine, self._h, int(k))
+
+    def coarse(self, k: int, u_first_new=None, want_defect: bool = True) -> float:
+        d = C.c_double(0.0)
+        inb = C.c_void_p(u_first_new.ptr) if u_first_new is not None else None
+        self.prop.call(L.lib().sp_parareal_window_coarse, self._h, int(k), inb, C.c_void_p(self.boundary.ptr),
+                       C.byref(d) if want_defect else None)
+        return d.value
+
+
+class DistributedParareal:
+    """Parareal over the ranks of a torch.distributed group, one slice window per rank.
+
+    Rank r owns slices slice_bounds(P, world, r).  Per iteration every rank
+    runs its fine sweep, receives the previous rank's boundary field, runs its
+    coarse sweep and sends its own boundary field to the next rank -- the
+    reference's pipelined ring (Parareal.h:116-165) with windows of slices
+    instead of single slices.  The window object provides begin/fine/coarse,
+    a `boundary` payload and `make_recv_buffer()`; fields travel as CUDA
+    tensors with NCCL and through host memory with gloo.
+    """
+
+    def __init__(self, window, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.w = window
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.gloo = dist.get_backend(group) == "gloo"
+
+    def _payload(self, field):
+        t = field.data if hasattr(field, "data") else field
+        return t.cpu() if (self.gloo and t.is_cuda) else t
+
+    def run(self, kmax: int, tol: float = 0.0):
+        """Runs up to kmax iterations (stops early once the max defect over all ranks is below tol).
+        Returns (iterations, per-iteration max defects)."""
+        import torch
+        dist, w = self.dist, self.w
+        w.begin()
+        recv_field = w.make_recv_buffer() if self.rank > 0 else None
+        defects = []
+        for k in range(kmax):
+            w.fine(k)
+            inbound = None
+            if self.rank > 0:
+                buf = self._payload(recv_field)
+                dist.recv(buf, src=self.rank - 1, group=self.group, tag=k)
+                if buf is not (recv_field.data if hasattr(recv_field, "data") else recv_field):
+                    (recv_field.data if hasattr(recv_field, "data") else recv_field).copy_(buf)
+                inbound = recv_field
+            d = w.coarse(k, inbound)
+            if self.rank < self.world - 1:
+                dist.send(self._payload(w.boundary), dst=self.rank + 1, group=self.group, tag=k)
+            t = torch.tensor([d], dtype=torch.float64)
+            if not self.gloo:
+                t = t.cuda()
+            dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+            defects.append(float(t.item()))
+            if tol > 0 and defects[-1] < tol:
+                return k + 1, defects
+        return kmax, defects
