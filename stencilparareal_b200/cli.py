@@ -1,0 +1,220 @@
+"""Command-line drivers with the reference's option names, on the B200 library.
+
+    python -m stencilparareal_b200.cli convection [--nu0 X --nufreq X --cx X --cy X --cz X
+                                                   --gridSize N --timeSteps N --endTime T --cfl C --order 1|4]
+        src/Convection/main.cpp: analytic initial field, DoRK4 (order 4) or DoEuler
+        (order 1) to endTime, "Total relative error" against the analytic solution.
+
+    python -m stencilparareal_b200.cli parareal --timeSlices P [--nu0 X --nufreq X --cx X --cy X --cz X
+        --gridSize N --endTime T --timeStepsFine N --timeStepsCoarse N --kmax K --noasync
+        --mode compare|serial|parallel|timing --coarse euler|rk4 --coarsePrecision f64|f32]
+        src/Parareal/main.cpp: the four run modes.  The slice count, which the
+        reference takes from the MPI communicator size, is --timeSlices; all slices
+        run on one GPU.  Energy comes from NVML (the reference reads Cray counters).
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import sys
+import time
+
+import numpy as np
+
+
+def _energy_j(device: int):
+    """Total energy of the GPU in joules from NVML, or None."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(device)
+        return pynvml.nvmlDeviceGetTotalEnergyConsumption(h) / 1000.0
+    except Exception:
+        return None
+
+
+def convection_config(argv):
+    """parseCommandLine of src/Convection/main.cpp:78-213 (defaults, --cfl logic)."""
+    ap = argparse.ArgumentParser(prog="convection")
+    for name in ("nu0", "nufreq", "cx", "cy", "cz", "endTime", "cfl"):
+        ap.add_argument("--" + name, type=float)
+    ap.add_argument("--gridSize", type=int)
+    ap.add_argument("--timeSteps", type=int)
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--mat", action="store_true")
+    a = ap.parse_args(argv)
+    if a.order not in (1, 4):
+        raise SystemExit(f"Order {a.order} is not supported")
+    c = dict(nu0=1.0, nufreq=0.0, cx=1.0, cy=1.0, cz=1.0, gridsize=32, timesteps=512, endtime=0.05, rk=a.order == 4)
+    for k in ("nu0", "nufreq", "cx", "cy", "cz"):
+        if getattr(a, k) is not None:
+            c[k] = getattr(a, k)
+    c["dx"] = 1.0 / c["gridsize"]
+    c["dt"] = c["endtime"] / c["timesteps"]
+    if a.endTime is not None:
+        c["endtime"] = a.endTime
+        c["dt"] = c["endtime"] / c["timesteps"]
+    if a.cfl is not None and a.gridSize is not None and a.timeSteps is not None:
+        raise SystemExit("Error: setting cfl, gridSize and timeSteps not allowed")
+    if a.gridSize is not None:
+        c["gridsize"] = a.gridSize
+        c["dx"] = 1.0 / c["gridsize"]
+    if a.timeSteps is not None:
+        c["timesteps"] = a.timeSteps
+        c["dt"] = c["endtime"] / c["timesteps"]
+    if a.cfl is not None:
+        if a.gridSize is not None:
+            dt = c["dx"] ** 2 * a.cfl / (1.5 * c["nu0"])
+            c["timesteps"] = int(c["endtime"] / dt + 0.5)
+            c["dt"] = c["endtime"] / c["timesteps"]
+        else:
+            dx = math.sqrt(c["dt"] * c["nu0"] / a.cfl)
+            c["gridsize"] = int(1.0 / dx + 0.5)
+            c["dx"] = 1.0 / c["gridsize"]
+    c["cfl"] = c["dt"] * 1.5 * c["nu0"] / (c["dx"] * c["dx"])
+    return c
+
+
+def run_convection(argv, out=sys.stdout) -> dict:
+    import stencilparareal_b200 as sp
+    from .solution import compute_error, fill_q
+    c = convection_config(argv)
+    n = c["gridsize"]
+    conv = sp.Convection(n, n, n, c["dx"], c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"])
+    q_in, q_out = conv.field(), conv.field()
+    conv.upload(q_in, fill_q(n, n, n, c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"], 0.0))
+    conv.synchronize()
+    t0 = time.perf_counter()
+    if c["rk"]:
+        conv.DoRK4(q_in, q_out, 0.0, c["dt"], c["timesteps"])
+    else:
+        conv.DoEuler(q_in, q_out, 0.0, c["dt"], c["timesteps"])
+    conv.synchronize()
+    elapsed = time.perf_counter() - t0
+    e_inf, x_inf, rel = compute_error(conv.download(q_out), c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"],
+                                      c["endtime"])
+    print(f"Grid: {n}^3, timesteps: {c['timesteps']}, dt: {c['dt']:g}, CFL: {c['cfl']:g}, "
+          f"order: {4 if c['rk'] else 1}", file=out)
+    print(f"Timing results:\n - total time: {elapsed * 1e3:.3f} msec\n", file=out)
+    print(f"Errors: exact={x_inf:g}, error={e_inf:g}", file=out)
+    print(f"\n Total relative error: {rel:g}", file=out)
+    return dict(c, error=rel, seconds=elapsed)
+
+
+def parareal_config(argv):
+    ap = argparse.ArgumentParser(prog="parareal")
+    ap.add_argument("--timeSlices", type=int, required=True)
+    for name in ("nu0", "nufreq", "cx", "cy", "cz", "endTime"):
+        ap.add_argument("--" + name, type=float)
+    for name in ("gridSize", "timeStepsFine", "timeStepsCoarse", "kmax"):
+        ap.add_argument("--" + name, type=int)
+    ap.add_argument("--mat", action="store_true")
+    ap.add_argument("--noasync", action="store_true")
+    ap.add_argument("--mode", default="compare")
+    ap.add_argument("--coarse", default="euler", choices=["euler", "rk4"])
+    ap.add_argument("--coarsePrecision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    from .parareal import RuntimeConfiguration
+    kw = {k: getattr(a, k) for k in ("nu0", "nufreq", "cx", "cy", "cz", "endTime", "gridSize", "timeStepsFine",
+                                     "timeStepsCoarse", "kmax") if getattr(a, k) is not None}
+    conf = RuntimeConfiguration(timeSlices=a.timeSlices, mat=a.mat, async_=not a.noasync, mode=a.mode, **kw)
+    return conf, a
+
+
+def run_parareal(argv, out=sys.stdout) -> dict:
+    import stencilparareal_b200 as sp
+    from .solution import error_reference, fill_q
+    conf, a = parareal_config(argv)
+    n, P = conf.gridSize(), conf.timeSlices()
+    print("Running with:\n"
+          f" - initial diffusion coefficient: {conf.nu0():g}\n"
+          f" - frequence of diffusion coefficient: {conf.nufreq():g}\n"
+          f" - advection velocity in x: {conf.cx():g}\n - advection velocity in y: {conf.cy():g}\n"
+          f" - advection velocity in z: {conf.cz():g}\n - spatial discretization step: {conf.dx():g}\n"
+          f" - endtime: {conf.endTime():g}\n - number of time slices: {P}\n"
+          f" - time slice size: {conf.timeSliceSize():g}\n - CFL fine: {conf.cflFine():g}\n"
+          f" - CFL coarse: {conf.cflCoarse():g}\n - timestep size fine: {conf.dtFine():g}\n"
+          f" - timestep size coarse: {conf.dtCoarse():g}\n"
+          f" - timesteps per slice fine propagator: {conf.timeStepsFinePerTimeSlice()}\n"
+          f" - timesteps per slice coarse propagator: {conf.timeStepsCoarsePerTimeSlice()}\n"
+          f" - parareal iterations: {conf.kmax()}\n"
+          f" - asynchronous communications: {'Enabled' if conf.async_() else 'Disabled'}\n", file=out)
+    conv = sp.Convection(n, n, n, conf.dx(), conf.nu0(), conf.nufreq(), conf.cx(), conf.cy(), conf.cz(),
+                         device=a.device)
+    q, qinitial, qref = conv.field(), conv.field(), conv.field()
+    par = sp.Parareal(conv, qinitial, q, 0.0, conf, coarse=a.coarse, coarse_precision=a.coarsePrecision)
+    q0 = fill_q(n, n, n, conf.nu0(), conf.nufreq(), conf.cx(), conf.cy(), conf.cz(), 0.0)
+    res = {"mode": conf.mode()}
+
+    def timed(fn):
+        conv.synchronize()
+        e0 = _energy_j(a.device)
+        t0 = time.perf_counter()
+        r = fn()
+        conv.synchronize()
+        dt = time.perf_counter() - t0
+        e1 = _energy_j(a.device)
+        return r, dt, (e1 - e0) if (e0 is not None and e1 is not None) else None
+
+    if conf.mode() == "compare":
+        # tau_F, tau_G and the speedup model (main.cpp:197-210)
+        _, tauF, _ = timed(lambda: conv.DoRK4(qinitial, qinitial, 0.0, conf.dtFine(),
+                                              4 * conf.timeStepsFinePerTimeSlice()))
+        _, tauG, _ = timed(lambda: conv.DoEuler(qinitial, qinitial, 0.0, conf.dtCoarse(),
+                                                4 * conf.timeStepsCoarsePerTimeSlice()))
+        max_speedup = sp.Parareal.max_speedup(tauG / tauF, conf.kmax(), P)
+        conv.upload(qinitial, q0)
+        _, t_serial, _ = timed(par.DoSerial)
+        qref.data.copy_(q.data)
+        conv.upload(qinitial, q0)
+        rep, t_par, _ = timed(par.DoParallel)
+        err = error_reference(conv.download(q), conv.download(qref))
+        print(f"\nSerial run time: {t_serial:g}\nParallel run time: {t_par:g}\nSpeedup: {t_serial / t_par:g}\n"
+              f"Maximal speedup: {max_speedup:g}\nError at end: {err:g}\n", file=out)
+        res.update(serial_s=t_serial, parallel_s=t_par, max_speedup=max_speedup, error=err)
+    elif conf.mode() == "serial":
+        conv.upload(qinitial, q0)
+        _, t, energy = timed(par.DoSerial)
+        print(f"\nSerial run time: {t:g}", file=out)
+        if energy is not None:
+            print(f"Device energy : {energy:f} J  ({energy / t:.3e} W)", file=out)
+        res.update(serial_s=t, energy_j=energy)
+    elif conf.mode() == "parallel":
+        conv.upload(qinitial, q0)
+        par.DoSerial()
+        print(" -- The serial computation is done", file=out)
+        qref.data.copy_(q.data)
+        conv.upload(qinitial, q0)
+        rep, t, energy = timed(par.DoParallel)
+        print(" -- The parallel computation is done", file=out)
+        err = error_reference(conv.download(q), conv.download(qref))
+        print(f"\nParallel run time: {t:f} s", file=out)
+        if energy is not None:
+            print(f"Device energy : {energy:f} J  ({energy / t:.3e} W)", file=out)
+        print(f"Error of parareal: {err:.4e}\n", file=out)
+        res.update(parallel_s=t, error=err, energy_j=energy)
+    else:  # timing (DoTimedParallel, Parareal.h:173-248): device times of the phases
+        conv.upload(qinitial, q0)
+        rep = par.DoParallel()
+        print("\nTimes:", file=out)
+        for label, v in (("total", rep["seconds"]), ("fine", rep["seconds_fine"]), ("coarse", rep["seconds_coarse"])):
+            print(f"{v:.6e}   {label}", file=out)
+        res.update(report=rep)
+    return res
+
+
+def main(argv=None):
+    argv = list(sys.argv[1:] if argv is None else argv)
+    if not argv or argv[0] not in ("convection", "parareal"):
+        print(__doc__)
+        return 2
+    if argv[0] == "convection":
+        run_convection(argv[1:])
+    else:
+        run_parareal(argv[1:])
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,40 @@
+"""CPU tests of the analytic-solution module and the CLI option handling."""
+import numpy as np
+
+from stencilparareal_b200 import solution as S
+from stencilparareal_b200.cli import convection_config, parareal_config
+
+
+def test_fill_q_matches_oracle(orc):
+    for n, args in ((8, (0.1, 0.0, 1.0, 1.0, 1.0, 0.0)), (6, (0.01, 100.0, 1.0, 0.5, 0.25, 0.05))):
+        nu0, nf, cx, cy, cz, t = args
+        mine = S.fill_q(n, n, n, nu0, nf, cx, cy, cz, t)
+        ref = orc.fillq(orc.params(n, nu0=nu0, nufreq=nf, cx=cx, cy=cy, cz=cz), t)
+        np.testing.assert_allclose(mine, ref, rtol=0, atol=1e-15)
+
+
+def test_error_measures(orc):
+    a = S.fill_q(8, 8, 8, 0.1, 0.0, 1, 1, 1, 0.01)
+    b = a + 1e-3 * np.sin(np.arange(a.size)).reshape(a.shape)
+    assert abs(S.error_reference(a, b) - orc.error_maxrel(a, b)) < 1e-16
+    e_inf, x_inf, rel = S.compute_error(b, 0.1, 0.0, 1, 1, 1, 0.01)
+    assert abs(rel - e_inf / x_inf) < 1e-16 and e_inf > 0
+
+
+def test_convection_options_follow_reference_rules():
+    # src/Convection/main.cpp:78-213: defaults, then --cfl picks the step count or the grid
+    c = convection_config([])
+    assert (c["gridsize"], c["timesteps"], c["endtime"], c["rk"]) == (32, 512, 0.05, True)
+    c = convection_config(["--gridSize", "64", "--cfl", "0.1", "--nu0", "0.1", "--endTime", "0.01"])
+    dt = (1 / 64) ** 2 * 0.1 / (1.5 * 0.1)
+    assert c["timesteps"] == int(0.01 / dt + 0.5)
+    c = convection_config(["--timeSteps", "100", "--cfl", "0.2", "--nu0", "0.5"])
+    assert c["gridsize"] == int(1 / np.sqrt(0.05 / 100 * 0.5 / 0.2) + 0.5)
+    assert convection_config(["--order", "1"])["rk"] is False
+
+
+def test_parareal_options():
+    conf, a = parareal_config(["--timeSlices", "32", "--gridSize", "128", "--endTime", "0.2", "--timeStepsFine",
+                               "20000", "--timeStepsCoarse", "200", "--noasync", "--mode", "Serial"])
+    assert conf.timeStepsCoarsePerTimeSlice() == 7 and conf.timeStepsFinePerTimeSlice() == 625
+    assert conf.mode() == "serial" and not conf.async_()

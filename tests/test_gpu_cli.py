@@ -1,0 +1,63 @@
+"""GPU tests of the command-line drivers and of the error paths of the C ABI."""
+import ctypes as C
+import io
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_convection_cli_converges_at_fourth_order():
+    from stencilparareal_b200.cli import run_convection
+    errs = []
+    for n in (16, 32):
+        r = run_convection(["--gridSize", str(n), "--timeSteps", "400", "--endTime", "0.02", "--nu0", "0.1"],
+                           out=io.StringIO())
+        errs.append(r["error"])
+    order = np.log2(errs[0] / errs[1])
+    assert 3.7 < order < 4.3, (errs, order)
+
+
+def test_parareal_cli_compare_mode_matches_oracle(orc):
+    from stencilparareal_b200.cli import run_parareal
+    out = io.StringIO()
+    r = run_parareal(["--timeSlices", "4", "--gridSize", "16", "--endTime", "0.02", "--timeStepsFine", "400",
+                      "--timeStepsCoarse", "32", "--nu0", "0.1", "--kmax", "2", "--noasync"], out=out)
+    assert "Error at end" in out.getvalue()
+    p = orc.params(16, nu0=0.1)
+    q, qs, em, el = orc.parareal(p, orc.parareal_cfg(0.02, 4, 400, 32, 2), orc.fillq(p, 0.0))
+    assert abs(r["error"] - em[-1]) <= 1e-6 * em[-1]
+    for mode in ("serial", "parallel", "timing"):
+        run_parareal(["--timeSlices", "4", "--gridSize", "12", "--endTime", "0.01", "--timeStepsFine", "40",
+                      "--timeStepsCoarse", "8", "--kmax", "2", "--mode", mode], out=io.StringIO())
+
+
+def test_error_paths_return_status(sp):
+    L = sp._lib
+    lib = L.lib()
+    c = sp.Convection(8, 8, 8, 0.125, 0.1, 0.0, 1, 1, 1)
+    f = c.field()
+    assert lib.sp_do_rk4(c.handle, None, C.c_void_p(f.ptr), 0.0, 1e-3, 1) == L.SP_ERR_INVALID
+    assert lib.sp_do_rk4(c.handle, C.c_void_p(f.ptr), C.c_void_p(f.ptr), 0.0, 1e-3, -1) == L.SP_ERR_INVALID
+    assert lib.sp_do_rk4(None, C.c_void_p(f.ptr), C.c_void_p(f.ptr), 0.0, 1e-3, 1) == L.SP_ERR_INVALID
+    assert lib.sp_set_tune(c.handle, 0, 1, 5, 8, 1) == L.SP_ERR_INVALID
+    p = L.SpParams(1, 8, 8, 0.125, 0.1, 0.0, 1, 1, 1, 1)
+    h = C.c_void_p()
+    assert lib.sp_convection_create(C.byref(p), 0, C.byref(h)) == L.SP_ERR_INVALID
+    cfg = L.SpPararealCfg()
+    cfg.endTime, cfg.timeSlices, cfg.timeStepsFine, cfg.timeStepsCoarse, cfg.kmax = 0.1, 0, 10, 10, 1
+    assert lib.sp_parareal_create(c.handle, C.byref(cfg), C.byref(h)) == L.SP_ERR_INVALID
+    cfg.timeSlices, cfg.first_slice, cfg.slice_count = 4, 3, 2
+    assert lib.sp_parareal_create(c.handle, C.byref(cfg), C.byref(h)) == L.SP_ERR_INVALID
+    # a window handle refuses the whole-problem entry point
+    conf = sp.RuntimeConfiguration(timeSlices=4, gridSize=8, endTime=0.01, timeStepsFine=8, timeStepsCoarse=4, kmax=1)
+    from stencilparareal_b200.parareal import WindowParareal
+    w = WindowParareal(c, f, c.field(), 0.0, conf, 0, 2)
+    with pytest.raises(sp.SpError):
+        w.DoParallel()
+    with pytest.raises(sp.SpError):  # a window that does not start at slice 0 needs the received field
+        w2 = WindowParareal(c, f, c.field(), 0.0, conf, 2, 2)
+        w2.begin()
+        w2.fine(0)
+        w2.coarse(0, None)
