@@ -128,7 +128,7 @@ def run_reference(args, rank, world):
     cores = os.cpu_count() or 1
     O.set_threads(cores)
     n = N_FINE
-    steps = 2  # bounded sample per step: 2 RK4 steps of the 256^3 workload
+    steps = 8  # bounded sample per step: 8 RK4 steps of the 256^3 workload (a few s on the host cores)
     p = O.params(n, dx=1.0 / n, nu0=NU, nufreq=0.0, cx=C[0], cy=C[1], cz=C[2])
     q = fourier_ic(n)
     for _ in range(args.warmup):
