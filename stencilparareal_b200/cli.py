@@ -1,16 +1,18 @@
 """Command-line drivers with the reference's option names, on the B200 library.
 
     python -m stencilparareal_b200.cli convection [--nu0 X --nufreq X --cx X --cy X --cz X
-                                                   --gridSize N --timeSteps N --endTime T --cfl C --order 1|4]
+                                                   --gridSize N --timeSteps N --endTime T --cfl C --order 1|4 --mat]
         src/Convection/main.cpp: analytic initial field, DoRK4 (order 4) or DoEuler
         (order 1) to endTime, "Total relative error" against the analytic solution.
 
     python -m stencilparareal_b200.cli parareal --timeSlices P [--nu0 X --nufreq X --cx X --cy X --cz X
         --gridSize N --endTime T --timeStepsFine N --timeStepsCoarse N --kmax K --noasync
-        --mode compare|serial|parallel|timing --coarse euler|rk4 --coarsePrecision f64|f32]
+        --mode compare|serial|parallel|timing --coarse euler|rk4 --coarsePrecision f64|f32 --mat]
         src/Parareal/main.cpp: the four run modes.  The slice count, which the
         reference takes from the MPI communicator size, is --timeSlices; all slices
         run on one GPU.  Energy comes from NVML (the reference reads Cray counters).
+
+    --mat writes the reference's MAT-v5 files into the working directory.
 """
 from __future__ import annotations
 
@@ -45,7 +47,8 @@ def convection_config(argv):
     a = ap.parse_args(argv)
     if a.order not in (1, 4):
         raise SystemExit(f"Order {a.order} is not supported")
-    c = dict(nu0=1.0, nufreq=0.0, cx=1.0, cy=1.0, cz=1.0, gridsize=32, timesteps=512, endtime=0.05, rk=a.order == 4)
+    c = dict(nu0=1.0, nufreq=0.0, cx=1.0, cy=1.0, cz=1.0, gridsize=32, timesteps=512, endtime=0.05, rk=a.order == 4,
+             mat=a.mat)
     for k in ("nu0", "nufreq", "cx", "cy", "cz"):
         if getattr(a, k) is not None:
             c[k] = getattr(a, k)
@@ -91,8 +94,27 @@ def run_convection(argv, out=sys.stdout) -> dict:
         conv.DoEuler(q_in, q_out, 0.0, c["dt"], c["timesteps"])
     conv.synchronize()
     elapsed = time.perf_counter() - t0
-    e_inf, x_inf, rel = compute_error(conv.download(q_out), c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"],
-                                      c["endtime"])
+    q_end = conv.download(q_out)
+    e_inf, x_inf, rel = compute_error(q_end, c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"], c["endtime"])
+    if c.get("mat"):
+        # src/Convection/main.cpp:311-327,351-355,393-405: init.mat, the cell "q" of
+        # convection_0_0_0.mat (the initial field), result_0_0_0.mat with the
+        # fields q (in), q (out), error and exact under the reference's names.
+        # The reference writes init.mat on every run; here only with --mat.
+        from .matfile import MatFile
+        q0 = conv.download(q_in)
+        exact = fill_q(n, n, n, c["nu0"], c["nufreq"], c["cx"], c["cy"], c["cz"], c["endtime"])
+        with MatFile("init.mat") as m:
+            m.addField("qIn", q0)
+        with MatFile("convection_0_0_0.mat") as m:
+            m.startCell("q", c["timesteps"])
+            m.addField(q0, 0)
+            m.endCell()
+        with MatFile("result_0_0_0.mat") as m:
+            m.addField("q", q0)
+            m.addField("q", q_end)
+            m.addField("error", q_end - exact)
+            m.addField("exact", exact)
     print(f"Grid: {n}^3, timesteps: {c['timesteps']}, dt: {c['dt']:g}, CFL: {c['cfl']:g}, "
           f"order: {4 if c['rk'] else 1}", file=out)
     print(f"Timing results:\n - total time: {elapsed * 1e3:.3f} msec\n", file=out)
@@ -172,6 +194,11 @@ def run_parareal(argv, out=sys.stdout) -> dict:
         err = error_reference(conv.download(q), conv.download(qref))
         print(f"\nSerial run time: {t_serial:g}\nParallel run time: {t_par:g}\nSpeedup: {t_serial / t_par:g}\n"
               f"Maximal speedup: {max_speedup:g}\nError at end: {err:g}\n", file=out)
+        if conf.mat():
+            from .matfile import MatFile
+            with MatFile("result.mat", conv) as m:  # main.cpp:251-253
+                m.addField("q", q)
+                m.addField("qreference", qref)
         res.update(serial_s=t_serial, parallel_s=t_par, max_speedup=max_speedup, error=err)
     elif conf.mode() == "serial":
         conv.upload(qinitial, q0)

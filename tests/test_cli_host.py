@@ -38,3 +38,26 @@ def test_parareal_options():
                                "20000", "--timeStepsCoarse", "200", "--noasync", "--mode", "Serial"])
     assert conf.timeStepsCoarsePerTimeSlice() == 7 and conf.timeStepsFinePerTimeSlice() == 625
     assert conf.mode() == "serial" and not conf.async_()
+
+
+def test_matfile_roundtrip(tmp_path):
+    import scipy.io
+    from stencilparareal_b200.matfile import MatFile
+    a = S.fill_q(6, 5, 4, 0.1, 0.0, 1, 1, 1, 0.0)  # shape (4, 5, 6)
+    b = (a * 2).astype(np.float32)
+    fn = str(tmp_path / "t.mat")
+    with MatFile(fn) as m:
+        m.addField("q", a)
+        m.addField("q", a, inc=3)
+        m.startCell("series", 2)
+        m.addField(a)
+        m.addField(b)
+        m.endCell()
+    d = scipy.io.loadmat(fn)
+    # MATLAB q(i, j, k) = interior cell (i, j, k): dims ni x nj x nk, i fastest
+    assert d["q"].shape == (6, 5, 4)
+    np.testing.assert_array_equal(d["q"], a.transpose(2, 1, 0))
+    np.testing.assert_array_equal(d["q_3"], a.transpose(2, 1, 0))
+    cell = d["series"]
+    assert cell.shape == (1, 2)
+    np.testing.assert_array_equal(cell[0, 1], b.transpose(2, 1, 0))

@@ -61,3 +61,24 @@ def test_error_paths_return_status(sp):
         w2.begin()
         w2.fine(0)
         w2.coarse(0, None)
+
+
+def test_mat_output_of_both_drivers(tmp_path, monkeypatch):
+    import scipy.io
+    from stencilparareal_b200.cli import run_convection, run_parareal
+    from stencilparareal_b200.solution import fill_q
+    monkeypatch.chdir(tmp_path)
+    run_convection(["--gridSize", "12", "--timeSteps", "40", "--endTime", "0.01", "--mat"], out=io.StringIO())
+    r = scipy.io.loadmat("result_0_0_0.mat")
+    exact = fill_q(12, 12, 12, 1.0, 0.0, 1, 1, 1, 0.01).transpose(2, 1, 0)
+    np.testing.assert_array_equal(r["exact"], exact)
+    np.testing.assert_allclose(r["q"] - exact, r["error"], rtol=0, atol=1e-15)
+    assert np.abs(r["error"]).max() < 1e-2 * np.abs(exact).max()
+    init = scipy.io.loadmat("init.mat")["qIn"]
+    np.testing.assert_array_equal(init, fill_q(12, 12, 12, 1.0, 0.0, 1, 1, 1, 0.0).transpose(2, 1, 0))
+    np.testing.assert_array_equal(scipy.io.loadmat("convection_0_0_0.mat")["q"][0, 0], init)
+    run_parareal(["--timeSlices", "4", "--gridSize", "12", "--endTime", "0.01", "--timeStepsFine", "40",
+                  "--timeStepsCoarse", "8", "--kmax", "4", "--mat"], out=io.StringIO())
+    m = scipy.io.loadmat("result.mat")
+    assert m["q"].shape == (12, 12, 12)
+    np.testing.assert_allclose(m["q"], m["qreference"], rtol=0, atol=1e-12)
