@@ -184,7 +184,8 @@ class Convection:
 
     # -- tuning ----------------------------------------------------------------
     def set_tune(self, precision: int, batch: int, ty: int, zchunk: int, kind: int):
-        """kind: 0 direct loads, 1 TMA/mbarrier pipeline."""
+        """kind: 0 direct loads, 1 TMA/mbarrier pipeline (single-stage kernels);
+        2 fused stage pairs for FP64 RK4 steps (ty 8 or 16)."""
         L.check(L.lib().sp_set_tune(self._h, precision, batch, ty, zchunk, int(kind)))
 
     def autotune(self, precision: int = L.SP_F64, batch: int = 1):
@@ -192,14 +193,15 @@ class Convection:
         return self.tuned_configs(precision, batch)
 
     def tuned_config(self, precision: int = L.SP_F64, batch: int = 1, op: int = 1):
-        """Launch shape of stage kernel `op` (0..3 RK4 S1..S4, 4 Euler)."""
+        """Launch shape of stage kernel `op` (0..3 RK4 S1..S4, 4 Euler; 9, 10 the
+        fused pairs 1+2 and 3+4, whose kind is 2 when RK4 steps run fused)."""
         ty, zc, tma = C.c_int(), C.c_int(), C.c_int()
         L.check(L.lib().sp_tuned_config(self._h, precision, batch, op, C.byref(ty), C.byref(zc), C.byref(tma)))
         return {"ty": ty.value, "zchunk": zc.value, "kind": tma.value}
 
     def tuned_configs(self, precision: int = L.SP_F64, batch: int = 1):
-        return {name: self.tuned_config(precision, batch, op)
-                for op, name in enumerate(("S1", "S2", "S3", "S4", "euler"))}
+        names = {0: "S1", 1: "S2", 2: "S3", 3: "S4", 4: "euler", 9: "P12", 10: "P34"}
+        return {name: self.tuned_config(precision, batch, op) for op, name in names.items()}
 
 
 def launch_count() -> int:

@@ -1,0 +1,498 @@
+// sp_fused.cu -- RK4 stages fused in pairs through shared memory.
+//
+// One low-storage RK4 step (src/Convection/Convection.cpp:286-327) is four
+// stencil stages.  Run one by one they move 16 field values per cell through
+// HBM (128 B in FP64).  Here stages 1+2 and stages 3+4 each run as one kernel:
+// the first stage of a pair is evaluated on the CTA tile widened by the
+// stencil radius (2 cells in x and y, 2 planes ahead in z) and kept in shared
+// memory, where the second stage reads it.  Per step the pairs move 7 values
+// per cell (56 B):
+//   pair 1+2: reads q;           writes y2 = q + dt/2 R(y1), acc = q + dt/6 k1 + dt/3 k2
+//   pair 3+4: reads y2, q, acc;  writes q' = acc + dt/3 k3 + dt/6 k4
+// Every value is computed with the same operations, in the same order, as the
+// single-stage kernels, so both paths give bit-identical fields.
+//
+// The widened first stage reads its input 4 cells beyond the tile, deeper
+// than the 2-cell halo of the caller's layout, so the pairs work on internal
+// fields with 4-cell periodic images (faces, edges and corners); the step's
+// input is widened once per propagation and the last step writes the
+// caller's layout directly.
+//
+// CTA: 32*TY threads; thread (warp w, lane l) owns cells (x0+2l, x0+2l+1) of
+// tile row y0+w (tile 64 x TY), and threads below NH also one 2-cell chunk of
+// the 2-cell ring around the tile.  The CTA marches a chunk of z-planes:
+// iteration v evaluates the first stage on plane z0-2+v and the second on
+// plane z0-4+v.  Shared memory: NSQ slots of the stencil input (TMA boxes of
+// (64+8) x (TY+8) cells), 3 slots of the widened first-stage field, NP slots
+// of pointwise operands (pair 3+4: q on the widened tile and acc on the tile),
+// and the mbarriers of the TMA slots.  z-neighbours of the thread's own cells
+// are carried in registers; the ring cells read theirs from the slots.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "sp_device.cuh"
+#include "sp_internal.h"
+#include "sp_stencil.cuh"
+
+namespace sp {
+
+namespace {
+
+using V2 = Vec<double, 2>;
+
+struct PairArgs {
+    long long item_stride, origin, px, plane;  // internal geometry (4-cell halo)
+    int ni, nj, nk, pz;
+    int tiles_x, zchunk;
+    const int* item_lo;
+    int item_base;
+    W13<double> w;
+    double c1y, c1a;   // first stage:  y = c1y k + base, a = c1a k + abase
+    double c2y, c2a;   // second stage
+    double* yout;      // pair 1+2: y2 (internal geometry, images 4 deep)
+    double* aout;      // pair 1+2: acc (internal geometry, interior only)
+    double* qout;      // pair 3+4: step result
+    long long o_item_stride, o_origin, o_px, o_plane;
+    int o_halo;        // image depth written with qout
+    int* err;
+};
+
+// Stores cells (x, x+1) of row (y, z) and every periodic image of them that
+// lies within `hd` cells of a face (faces, edges and corners).  base: the
+// item's interior origin; x < ni.  The cell itself is one 16-byte store; the
+// x-images of the row are a short branch taken by the lanes at the x faces,
+// and the copies of the row into the y/z halo a longer one taken only on the
+// rows and planes next to those faces.
+__device__ __forceinline__ void row_pair(double* row, int ni, int hd, int x, const V2& v) {
+    if (x + 2 <= ni) st16<double>(row + x, v);
+    else row[x] = v.v[0];
+    if (x < hd || x + 2 > ni - hd) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int xe = x + e;
+            if (xe >= ni) continue;
+            if (xe < hd) row[xe + ni] = v.v[e];
+            if (xe >= ni - hd) row[xe - ni] = v.v[e];
+        }
+    }
+}
+
+__device__ __forceinline__ void store_pair(double* base, long long px, long long plane, int ni, int nj, int nk,
+                                           int hd, int x, int y, int z, const V2& v) {
+    double* row = base + (long long)z * plane + (long long)y * px;
+    row_pair(row, ni, hd, x, v);
+    if (y < hd || y >= nj - hd || z < hd || z >= nk - hd) {
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            if (iz == 1 && !(z < hd)) continue;
+            if (iz == 2 && !(z >= nk - hd)) continue;
+            const long long oz = iz == 0 ? 0 : (iz == 1 ? (long long)nk * plane : -(long long)nk * plane);
+#pragma unroll
+            for (int iy = 0; iy < 3; ++iy) {
+                if (iz == 0 && iy == 0) continue;  // the row itself
+                if (iy == 1 && !(y < hd)) continue;
+                if (iy == 2 && !(y >= nj - hd)) continue;
+                const long long oy = iy == 0 ? 0 : (iy == 1 ? (long long)nj * px : -(long long)nj * px);
+                row_pair(row + oz + oy, ni, hd, x, v);
+            }
+        }
+    }
+}
+
+// R4 of cells (pos, pos+1) of a slot of row width W; the centre values and
+// the z-neighbours are given, the x- and y-neighbours are read from the slot.
+template <int W>
+__device__ __forceinline__ void rhs_c(const W13<double>& wt, const double* C, int pos, const V2& cen,
+                                      const V2& zm2, const V2& zm1, const V2& zp1, const V2& zp2, double k[2]) {
+    const V2 r0 = ld16<double>(C + pos - 2), r2 = ld16<double>(C + pos + 2);
+    const V2 ym2 = ld16<double>(C + pos - 2 * W), ym1 = ld16<double>(C + pos - W);
+    const V2 yp1 = ld16<double>(C + pos + W), yp2 = ld16<double>(C + pos + 2 * W);
+    const double row[6] = {r0.v[0], r0.v[1], cen.v[0], cen.v[1], r2.v[0], r2.v[1]};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        Nb<double> s;
+        s.c = row[2 + e];
+        s.xm1 = row[1 + e]; s.xp1 = row[3 + e];
+        s.xm2 = row[e]; s.xp2 = row[4 + e];
+        s.ym1 = ym1.v[e]; s.yp1 = yp1.v[e]; s.ym2 = ym2.v[e]; s.yp2 = yp2.v[e];
+        s.zm1 = zm1.v[e]; s.zp1 = zp1.v[e]; s.zm2 = zm2.v[e]; s.zp2 = zp2.v[e];
+        k[e] = rhs_w13(wt, s);
+    }
+}
+
+template <int TY, int NSQ, int NP, int PAIR>
+struct PairShape {
+    static constexpr int TX = 64;
+    static constexpr int WB = TX + 8, HB = TY + 8;  // stencil-input slot (box at x0-4, y0-4)
+    static constexpr int WE = TX + 4, HE = TY + 4;  // widened first-stage slot (origin x0-2, y0-2)
+    static constexpr int SB = WB * HB, SE = WE * HE, SA = TX * TY;
+    static constexpr int NE = 3;
+    static constexpr int NHR = 4 * (TX / 2);        // ring chunks in the two rows above and below (x0 .. x0+63)
+    static constexpr int NH = NHR + 2 * TY;         // plus the two columns left and right
+    static constexpr int SP = PAIR == 1 ? SE + SA : 0;
+    static constexpr size_t smem = 128 + (size_t)(NSQ * SB + NE * SE + NP * SP) * 8 + (NSQ + NP) * 8;
+};
+
+template <int PAIR, int TY, int NSQ, int NP>
+__global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
+    k_rk4_pair(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_q,
+               const __grid_constant__ CUtensorMap tm_a, const PairArgs a) {
+    using S = PairShape<TY, NSQ, NP, PAIR>;
+    constexpr int TX = S::TX, WB = S::WB, WE = S::WE, SB = S::SB, SE = S::SE, SP = S::SP;
+    constexpr int NE = S::NE, NHR = S::NHR, NH = S::NH;
+    constexpr uint32_t SBYTES = SB * 8, PBYTES = SP * 8;
+    static_assert(SBYTES % 128 == 0 && (SE * 8) % 128 == 0 && (S::SA * 8) % 128 == 0, "slot alignment");
+    static_assert(NH <= 32 * TY, "ring chunks per CTA");
+    static_assert(NSQ >= 6, "five stencil planes in use plus one in flight");
+
+    extern __shared__ unsigned char smem_raw[];
+    double* sb = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    double* es = sb + NSQ * SB;
+    double* ps = es + NE * SE;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ps + NP * SP);
+
+    const int b = blockIdx.z;
+    if (a.item_lo && b + a.item_base < *a.item_lo) return;
+    const int x0 = (blockIdx.x % a.tiles_x) * TX;
+    const int y0 = (blockIdx.x / a.tiles_x) * TY;
+    const int z0 = blockIdx.y * a.zchunk;
+    const int z1 = min(z0 + a.zchunk, a.nk);
+    const int nv = z1 - z0 + 4;  // first-stage planes z0-2 .. z1+1
+    const int nu = z1 - z0 + 8;  // stencil planes z0-4 .. z1+3
+    const int zs = b * a.pz + z0;  // tensor-map plane of stencil plane 0 (interior z0-4)
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const bool leader = tid == 0;
+
+    if (leader) {
+        prefetch_tensormap(&tm_s);
+#pragma unroll
+        for (int i = 0; i < NSQ + NP; ++i) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    // stencil plane u -> slot u % NSQ; pointwise plane v -> slot v % NP
+    auto issue_s = [&](int u) {
+        const int s = u % NSQ;
+        mbar_arrive_expect_tx(&bar[s], SBYTES);
+        tma_load_3d(sb + s * SB, &tm_s, x0, y0, zs + u, &bar[s]);  // interior (x0-4, y0-4)
+    };
+    auto issue_p = [&](int v) {
+        const int s = v % NP;
+        mbar_arrive_expect_tx(&bar[NSQ + s], PBYTES);
+        double* d = ps + s * SP;
+        tma_load_3d(d, &tm_q, x0 + 2, y0 + 2, zs + 2 + v, &bar[NSQ + s]);       // q, interior (x0-2, y0-2)
+        tma_load_3d(d + SE, &tm_a, x0 + 4, y0 + 4, zs + 2 + v, &bar[NSQ + s]);  // acc, interior (x0, y0)
+    };
+    int s_hi = -1, p_hi = -1;  // highest planes issued (leader)
+    if (leader) {
+        for (int u = 0; u < NSQ && u < nu; ++u) { issue_s(u); s_hi = u; }
+        if constexpr (PAIR == 1)
+            for (int v = 0; v < NP && v < nv; ++v) { issue_p(v); p_hi = v; }
+    }
+    auto drain = [&](int s_done, int p_done) {
+        if (!leader) return;
+        for (int u = s_done + 1; u <= s_hi; ++u) (void)mbar_wait_bounded(&bar[u % NSQ], (uint32_t)((u / NSQ) & 1));
+        for (int v = p_done + 1; v <= p_hi; ++v)
+            (void)mbar_wait_bounded(&bar[NSQ + v % NP], (uint32_t)((v / NP) & 1));
+    };
+
+    // own cells and ring chunk
+    const int m_s = (w + 4) * WB + 2 * lane + 4;
+    const int m_e = (w + 2) * WE + 2 * lane + 2;
+    const bool has_h = tid < NH;
+    // the ring: rows y0-2, y0-1, y0+TY, y0+TY+1 over the tile's columns, and
+    // columns x0-2..x0-1, x0+64..x0+65 over the tile's rows (the corners are
+    // not operands of the second stage)
+    int hex = 0, hey = 0;
+    if (tid < NHR) {
+        const int r = tid >> 5;
+        hey = r < 2 ? r : TY + r;
+        hex = 2 + 2 * (tid & 31);
+    } else if (has_h) {
+        const int d = tid - NHR;
+        hey = 2 + (d >> 1);
+        hex = (d & 1) ? WE - 2 : 0;
+    }
+    const int h_s = (hey + 2) * WB + hex + 2;
+    const int h_e = hey * WE + hex;
+
+    bool bad = false;
+    // Register windows of the own cells, indexed by plane mod 5 so that the
+    // loop, unrolled by 5, renames registers instead of moving them:
+    //   qw[u % 5]: stencil input at stencil plane u (planes v .. v+4 live)
+    //   ew[p % 5]: first-stage value at first-stage plane p (p = v-4 .. v)
+    //   aw[p % 5]: first-stage accumulator partial (p = v-2 .. v)
+    V2 qw[5], ew[5], aw[5];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {  // prologue: stencil planes 0..3
+        if (!mbar_wait_bounded(&bar[u], 0)) bad = true;
+        qw[u] = ld16<double>(sb + u * SB + m_s);
+    }
+#pragma unroll
+    for (int u = 0; u < 5; ++u) ew[u] = aw[u] = V2{};
+
+    const int x = x0 + 2 * lane;
+    const int y = y0 + w;
+    const bool live = x < a.ni && y < a.nj;
+    const long long ob = (long long)b * a.item_stride + a.origin;
+    double* const ybase = a.yout ? a.yout + ob : nullptr;
+    double* arow = nullptr;
+    if constexpr (PAIR == 0) arow = a.aout + ob + (long long)(z0 - 4) * a.plane + (long long)y * a.px + x;
+    double* const obase = PAIR == 1 ? a.qout + (long long)b * a.o_item_stride + a.o_origin : nullptr;
+
+    int s_v = 0;                    // slot of stencil plane v
+    int s_4 = 4 % NSQ;              // slot and phase of stencil plane v+4
+    uint32_t ph_4 = (4 / NSQ) & 1;
+    int e_v = 0;                    // slot of first-stage plane v (mod 3)
+    int sp_v = 0;                   // pointwise slot and phase of plane v
+    uint32_t ph_p = 0;
+
+    // One plane iteration; K = v mod 5.  Returns false when the CTA must stop.
+    auto iterate = [&](auto kc, int v) -> bool {
+        constexpr int K = decltype(kc)::value;
+        if (!mbar_wait_bounded(&bar[s_4], ph_4)) bad = true;
+        auto slot = [&](int k) {
+            int s = s_v + k;
+            if (s >= NSQ) s -= NSQ;
+            return sb + s * SB;
+        };
+        const double* P0 = slot(0);
+        const double* P1 = slot(1);
+        const double* P2 = slot(2);
+        const double* P3 = slot(3);
+        const double* P4 = slot(4);
+        qw[(K + 4) % 5] = ld16<double>(P4 + m_s);
+        const double* PW = nullptr;
+        if constexpr (PAIR == 1) {
+            if (!mbar_wait_bounded(&bar[NSQ + sp_v], ph_p)) bad = true;
+            PW = ps + sp_v * SP;
+        }
+        double* E = es + e_v * SE;
+        (void)PW;
+
+        // first stage, own cells (first-stage plane v, stencil centre v+2;
+        // the centre value is the window's)
+        {
+            double k[2];
+            rhs_c<WB>(a.w, P2, m_s, qw[(K + 2) % 5], qw[K], qw[(K + 1) % 5], qw[(K + 3) % 5], qw[(K + 4) % 5], k);
+            V2 en, an;
+            if constexpr (PAIR == 0) {
+                const V2& c = qw[(K + 2) % 5];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    en.v[e] = fmaT(a.c1y, k[e], c.v[e]);
+                    an.v[e] = fmaT(a.c1a, k[e], c.v[e]);
+                }
+            } else {
+                const V2 qv = ld16<double>(PW + m_e);
+                const V2 av = ld16<double>(PW + SE + w * TX + 2 * lane);
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    en.v[e] = fmaT(a.c1y, k[e], qv.v[e]);
+                    an.v[e] = fmaT(a.c1a, k[e], av.v[e]);
+                }
+            }
+            st16<double>(E + m_e, en);
+            ew[K] = en;
+            aw[K] = an;
+        }
+        // first stage, ring chunk
+        if (has_h) {
+            const V2 zm2 = ld16<double>(P0 + h_s), zm1 = ld16<double>(P1 + h_s);
+            const V2 zp1 = ld16<double>(P3 + h_s), zp2 = ld16<double>(P4 + h_s);
+            const V2 cen = ld16<double>(P2 + h_s);
+            V2 hv;
+            double k[2];
+            rhs_c<WB>(a.w, P2, h_s, cen, zm2, zm1, zp1, zp2, k);
+            V2 base = cen;
+            if constexpr (PAIR == 1) base = ld16<double>(PW + h_e);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) hv.v[e] = fmaT(a.c1y, k[e], base.v[e]);
+            st16<double>(E + h_e, hv);
+        }
+        // second stage on plane z0-4+v (first-stage plane v-2, stencil plane v)
+        if (v >= 4) {
+            const int ez = e_v == 2 ? 0 : e_v + 1;  // slot of first-stage plane v-2
+            double k[2];
+            rhs_c<WE>(a.w, es + ez * SE, m_e, ew[(K + 3) % 5], ew[(K + 1) % 5], ew[(K + 2) % 5], ew[(K + 4) % 5],
+                      ew[K], k);
+            const V2& ap = aw[(K + 3) % 5];
+            V2 o;
+            [[maybe_unused]] V2 oa;
+            if constexpr (PAIR == 0) {
+                const V2& qc = qw[K];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    o.v[e] = fmaT(a.c2y, k[e], qc.v[e]);
+                    oa.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 2; ++e) o.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
+            }
+            if (live) {
+                const int z = z0 - 4 + v;
+                if constexpr (PAIR == 0) {
+                    store_pair(ybase, a.px, a.plane, a.ni, a.nj, a.nk, 4, x, y, z, o);
+                    if (x + 2 <= a.ni) st16<double>(arow, oa);
+                    else arow[0] = oa.v[0];
+                } else {
+                    store_pair(obase, a.o_px, a.o_plane, a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
+                }
+            }
+        }
+        if constexpr (PAIR == 0) arow += a.plane;  // plane z0-4+v -> next
+        if (__syncthreads_or(bad)) {
+            if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+            drain(v + 4, v);
+            return false;
+        }
+        if (leader) {
+            fence_proxy_async_smem();
+            if (v + NSQ < nu) { issue_s(v + NSQ); s_hi = v + NSQ; }
+            if constexpr (PAIR == 1)
+                if (v + NP < nv) { issue_p(v + NP); p_hi = v + NP; }
+        }
+        if (++s_v == NSQ) s_v = 0;
+        if (++s_4 == NSQ) { s_4 = 0; ph_4 ^= 1u; }
+        if (++e_v == 3) e_v = 0;
+        if constexpr (PAIR == 1)
+            if (++sp_v == NP) { sp_v = 0; ph_p ^= 1u; }
+        return true;
+    };
+
+    for (int vb = 0; vb < nv; vb += 5) {  // nv is uniform over the CTA
+        if (!iterate(std::integral_constant<int, 0>{}, vb)) return;
+        if (vb + 1 < nv && !iterate(std::integral_constant<int, 1>{}, vb + 1)) return;
+        if (vb + 2 < nv && !iterate(std::integral_constant<int, 2>{}, vb + 2)) return;
+        if (vb + 3 < nv && !iterate(std::integral_constant<int, 3>{}, vb + 3)) return;
+        if (vb + 4 < nv && !iterate(std::integral_constant<int, 4>{}, vb + 4)) return;
+    }
+}
+
+
+
+// ---------------------------------------------------------------------------
+// Widening: interior of a caller-layout field -> internal field with every
+// periodic image within 4 cells of a face.
+__global__ void k_widen(double* dst, Geo gd, const double* src, Geo gs, int items, const int* item_lo,
+                        int item_base) {
+    const long long n = (long long)gd.ni * gd.nj * gd.nk;
+    const int b = blockIdx.y;
+    if (item_lo && b + item_base < *item_lo) return;
+    const double* sb = src + (long long)b * gs.total + gs.origin;
+    double* db = dst + (long long)b * gd.total + gd.origin;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % gd.ni);
+        const int y = (int)((t / gd.ni) % gd.nj);
+        const int z = (int)(t / ((long long)gd.ni * gd.nj));
+        const double v = sb[(long long)z * gs.plane + (long long)y * gs.px + x];
+        const int hd = gd.halo;
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            if (iz == 1 && !(z < hd)) continue;
+            if (iz == 2 && !(z >= gd.nk - hd)) continue;
+            const int zz = iz == 0 ? z : (iz == 1 ? z + gd.nk : z - gd.nk);
+#pragma unroll
+            for (int iy = 0; iy < 3; ++iy) {
+                if (iy == 1 && !(y < hd)) continue;
+                if (iy == 2 && !(y >= gd.nj - hd)) continue;
+                const int yy = iy == 0 ? y : (iy == 1 ? y + gd.nj : y - gd.nj);
+                double* r = db + (long long)zz * gd.plane + (long long)yy * gd.px;
+                r[x] = v;
+                if (x < hd) r[x + gd.ni] = v;
+                if (x >= gd.ni - hd) r[x - gd.ni] = v;
+            }
+        }
+    }
+}
+
+template <int PAIR, int TY, int NSQ, int NP>
+cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, const Shape& sh, cudaStream_t s,
+                          int* err) {
+    using S = PairShape<TY, NSQ, NP, PAIR>;
+    CUtensorMap ts{}, tq{}, ta{};
+    if (!make_tmap(&ts, g4, PAIR == 0 ? L.q : L.y2, L.items, S::WB, S::HB)) return cudaErrorInvalidValue;
+    if (PAIR == 1) {
+        if (!make_tmap(&tq, g4, L.q, L.items, S::WE, S::HE)) return cudaErrorInvalidValue;
+        if (!make_tmap(&ta, g4, L.acc, L.items, S::TX, TY)) return cudaErrorInvalidValue;
+    }
+    PairArgs a{};
+    a.item_stride = g4.total; a.origin = g4.origin; a.px = g4.px; a.plane = g4.plane;
+    a.ni = g4.ni; a.nj = g4.nj; a.nk = g4.nk; a.pz = (int)g4.pz;
+    a.tiles_x = (g4.ni + S::TX - 1) / S::TX;
+    const int tiles_y = (g4.nj + TY - 1) / TY;
+    a.zchunk = sh.zchunk;
+    const int nzc = (g4.nk + sh.zchunk - 1) / sh.zchunk;
+    a.item_lo = L.item_lo;
+    a.item_base = L.item_base;
+    fill_w13<double>(a.w, L.coef, L.nu);
+    const double dthalf = L.dt * .5;
+    if (PAIR == 0) {  // the coefficients of stages 1 and 2 of the single-stage path
+        a.c1y = dthalf; a.c1a = L.dt / 6.; a.c2y = dthalf; a.c2a = L.dt / 3.;
+        a.yout = static_cast<double*>(L.y2);
+        a.aout = static_cast<double*>(L.acc);
+    } else {          // stages 3 and 4
+        a.c1y = L.dt; a.c1a = L.dt / 3.; a.c2a = L.dt / 6.;
+        a.qout = static_cast<double*>(L.out);
+        a.o_item_stride = go.total; a.o_origin = go.origin; a.o_px = go.px; a.o_plane = go.plane;
+        a.o_halo = go.halo;
+    }
+    a.err = err;
+    dim3 grid(a.tiles_x * tiles_y, nzc, L.items);
+    if (grid.y > 65535u || grid.z > 65535u) return cudaErrorInvalidConfiguration;
+    k_rk4_pair<PAIR, TY, NSQ, NP><<<grid, 32 * TY, S::smem, s>>>(ts, tq, ta, a);
+    return cudaGetLastError();
+}
+
+template <int PAIR, int TY, int NSQ, int NP>
+cudaError_t set_pair_attr() {
+    return cudaFuncSetAttribute(k_rk4_pair<PAIR, TY, NSQ, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)PairShape<TY, NSQ, NP, PAIR>::smem);
+}
+
+unsigned grid_cells(long long n) {
+    const long long b = (n + 255) / 256;
+    return (unsigned)(b < 148 * 16 ? b : 148 * 16);
+}
+
+}  // namespace
+
+bool pair_supported(const Geo& g) { return g.es == 8 && g.ni >= 4 && g.nj >= 4 && g.nk >= 4; }
+
+cudaError_t prepare_pairs() {
+    cudaError_t e = set_pair_attr<0, 8, 7, 2>();
+    if (e == cudaSuccess) e = set_pair_attr<1, 8, 7, 2>();
+    if (e == cudaSuccess) e = set_pair_attr<0, 16, 7, 2>();
+    if (e == cudaSuccess) e = set_pair_attr<1, 16, 7, 2>();
+    return e;
+}
+
+cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const Shape& sh, cudaStream_t s,
+                        int* err) {
+    add_launches(1);
+    if (!pair_supported(g4) || g4.halo != 4 || sh.zchunk < 1) return cudaErrorInvalidValue;
+    if (L.pair == 0) {
+        if (sh.ty == 8) return launch_pair_T<0, 8, 7, 2>(g4, go, L, sh, s, err);
+        if (sh.ty == 16) return launch_pair_T<0, 16, 7, 2>(g4, go, L, sh, s, err);
+    } else {
+        if (sh.ty == 8) return launch_pair_T<1, 8, 7, 2>(g4, go, L, sh, s, err);
+        if (sh.ty == 16) return launch_pair_T<1, 16, 7, 2>(g4, go, L, sh, s, err);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* src, int items, const int* item_lo,
+                         int item_base, cudaStream_t s) {
+    add_launches(1);
+    if (g4.es != 8 || gs.es != 8 || items < 1 || items > 65535) return cudaErrorInvalidValue;
+    dim3 grid(grid_cells((long long)g4.ni * g4.nj * g4.nk), items);
+    k_widen<<<grid, 256, 0, s>>>(static_cast<double*>(dst), g4, static_cast<const double*>(src), gs, items, item_lo,
+                                 item_base);
+    return cudaGetLastError();
+}
+
+}  // namespace sp

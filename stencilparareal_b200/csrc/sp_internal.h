@@ -9,12 +9,15 @@ namespace sp {
 // Geometry of one field in HBM (see sp_field_layout in include/sp_abi.h).
 struct Geo {
     int ni = 0, nj = 0, nk = 0;
-    int lx = 0;         // columns left of interior i = 0 (16 bytes worth)
+    int lx = 0;         // columns left of interior i = 0 (a multiple of 16 bytes, >= halo)
     int es = 0;         // element size in bytes
+    int halo = 2;       // periodic image depth in y and z (and at least this much in x)
     long long px = 0, py = 0, pz = 0, plane = 0, origin = 0, total = 0;
 };
 
-Geo make_geo(int ni, int nj, int nk, int es);
+// halo 2: the caller-visible layout of sp_field_layout.  halo 4: internal
+// fields of the fused stage pairs.
+Geo make_geo(int ni, int nj, int nk, int es, int halo = 2);
 
 // Kernel families.
 enum Op : int {
@@ -38,6 +41,8 @@ struct Shape {
 constexpr int kNumOps = OP_ADJ + 4;
 struct Tune {
     Shape op[kNumOps];
+    Shape pair[2];    // fused stage pairs 1+2 and 3+4 (ty 8 or 16)
+    int fused = 0;    // 1: FP64 RK4 steps run as the two fused pairs
     void set_all(const Shape& s) {
         for (auto& o : op) o = s;
     }
@@ -85,6 +90,30 @@ struct StageLaunch {
 
 // Launches one stage kernel; counts the launch.  err: device error word.
 cudaError_t launch_stage(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err);
+
+// Fused RK4 stage pairs (sp_fused.cu) on internal FP64 fields of geometry g4
+// (make_geo(..., 8, 4)).  Pair 0 (stages 1+2): reads q; writes y2 (with
+// images) and acc.  Pair 1 (stages 3+4): reads y2, q and acc; writes the step
+// result to `out` in geometry go (g4, with out == acc allowed, or the caller's
+// layout), with periodic images go.halo deep.
+struct PairLaunch {
+    int pair = 0;
+    const void* q = nullptr;
+    void* y2 = nullptr;
+    void* acc = nullptr;
+    void* out = nullptr;
+    int items = 1;
+    const int* item_lo = nullptr;    // as in StageLaunch
+    int item_base = 0;
+    double nu = 0, dt = 0;
+    Coef coef;
+};
+bool pair_supported(const Geo& g);  // FP64, at least 4 interior cells per dimension
+cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const Shape& sh, cudaStream_t s, int* err);
+// dst (geometry g4) <- interior of src (geometry gs), with g4.halo-deep images (FP64, items fields).
+cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* src, int items, const int* item_lo,
+                         int item_base, cudaStream_t s);
+cudaError_t prepare_pairs();
 
 // Pointwise helpers.
 cudaError_t launch_periodicity(const Geo& g, void* field, int items, cudaStream_t s);

@@ -42,6 +42,7 @@
 
 #include "sp_device.cuh"
 #include "sp_internal.h"
+#include "sp_stencil.cuh"
 
 namespace sp {
 
@@ -51,16 +52,16 @@ std::atomic<long long> g_launches{0};
 long long launches() { return g_launches.load(); }
 void add_launches(long long n) { g_launches += n; }
 
-Geo make_geo(int ni, int nj, int nk, int es) {
+Geo make_geo(int ni, int nj, int nk, int es, int halo) {
     Geo g;
-    g.ni = ni; g.nj = nj; g.nk = nk; g.es = es;
-    g.lx = 16 / es;
+    g.ni = ni; g.nj = nj; g.nk = nk; g.es = es; g.halo = halo;
+    g.lx = (halo * es + 15) / 16 * 16 / es;
     const long long need = (long long)ni + 2 * g.lx;
     g.px = (need + 31) / 32 * 32;
-    g.py = nj + 4;
-    g.pz = nk + 4;
+    g.py = nj + 2 * halo;
+    g.pz = nk + 2 * halo;
     g.plane = g.px * g.py;
-    g.origin = 2 * g.plane + 2 * g.px + g.lx;
+    g.origin = halo * g.plane + halo * g.px + g.lx;
     g.total = g.plane * g.pz;
     return g;
 }
@@ -84,14 +85,6 @@ Coef make_coef(double dx, double cx, double cy, double cz, int upwind) {
     c.dx = dx;
     return c;
 }
-
-// ---------------------------------------------------------------------------
-// R4 as 13 per-offset weights of the reference's coefficients:
-//   ca_d (8(q[-1]-q[+1]) - (q[-2]-q[+2])) + nl (16 S1 - S2 - 90 q).
-template <typename T>
-struct W13 {
-    T m1[3], p1[3], m2[3], p2[3], c;
-};
 
 // Kernel arguments.
 template <typename T>
@@ -132,11 +125,6 @@ struct OpTraits {
     static constexpr bool writes_a = (OP == OP_RK_S1 || OP == OP_RK_S2 || OP == OP_RK_S3 || OP == OP_ADJ + 0 ||
                                       OP == OP_ADJ + 1 || OP == OP_ADJ + 2);
     static constexpr bool adjoint = OP >= OP_ADJ;
-};
-
-template <typename T>
-struct Nb {
-    T c, xm1, xp1, xm2, xp2, ym1, yp1, ym2, yp2, zm1, zp1, zm2, zp2;
 };
 
 template <typename T>
@@ -327,13 +315,6 @@ __global__ void __launch_bounds__(32 * TYD) k_stage_direct(const KArgs<T> a) {
 // away from every x/y face skip the periodic-image logic except on the four
 // planes next to the z faces.
 
-template <typename T>
-__device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
-    const T sx = fmaT(w.m2[0], s.xm2, fmaT(w.m1[0], s.xm1, fmaT(w.p1[0], s.xp1, w.p2[0] * s.xp2)));
-    const T sy = fmaT(w.m2[1], s.ym2, fmaT(w.m1[1], s.ym1, fmaT(w.p1[1], s.yp1, w.p2[1] * s.yp2)));
-    const T sz = fmaT(w.m2[2], s.zm2, fmaT(w.m1[2], s.zm1, fmaT(w.p1[2], s.zp1, w.p2[2] * s.zp2)));
-    return fmaT(w.c, s.c, (sx + sy) + sz);
-}
 
 template <typename T, int OP, int TY, int NS, int NP>
 __global__ void __launch_bounds__(32 * TY)
@@ -550,8 +531,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// Tensor map over `items` fields of geometry g starting at `base`: dims
-// (px, py, pz*items), box (bw, bh, 1).
+}  // namespace
+
 bool make_tmap(CUtensorMap* tm, const Geo& g, const void* base, int items, int bw, int bh) {
     auto enc = encode_fn();
     if (!enc || !base) return false;
@@ -565,6 +546,8 @@ bool make_tmap(CUtensorMap* tm, const Geo& g, const void* base, int items, int b
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
+
+namespace {
 
 template <typename T>
 KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err) {
@@ -585,17 +568,7 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err)
     a.lap_scale = (L.op == OP_EULER) ? c.s2 : c.s4;
     a.c_y = (T)L.c_y; a.c_acc = (T)L.c_acc;
     a.err = err;
-    {
-        // RHS4 as per-offset weights (used by the TMA RK stages; one nu per launch)
-        const double nl = L.nu * c.s4;
-        for (int d = 0; d < 3; ++d) {
-            a.w.m1[d] = (T)(8. * c.ca[d] + 16. * nl);
-            a.w.p1[d] = (T)(-8. * c.ca[d] + 16. * nl);
-            a.w.m2[d] = (T)(-c.ca[d] - nl);
-            a.w.p2[d] = (T)(c.ca[d] - nl);
-        }
-        a.w.c = (T)(-90. * nl);
-    }
+    fill_w13<T>(a.w, c, L.nu);  // RHS4 as per-offset weights (TMA RK stages; one nu per launch)
     switch (L.op) {
         case OP_RK_S1: a.aout = (T*)L.acc; break;
         case OP_RK_S2:
@@ -730,6 +703,7 @@ cudaError_t prepare_kernels() {
     chk(set_attr_op<float, OP_RK_S1>()); chk(set_attr_op<float, OP_RK_S2>());
     chk(set_attr_op<float, OP_RK_S3>()); chk(set_attr_op<float, OP_RK_S4>());
     chk(set_attr_op<float, OP_EULER>());
+    chk(prepare_pairs());
     return e;
 }
 

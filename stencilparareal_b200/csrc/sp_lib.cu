@@ -96,10 +96,13 @@ struct sp_convection {
     sp_params P{};
     int device = 0;
     Geo g[2];          // [0] FP64, [1] FP32
+    Geo g4;            // FP64 with 4-cell halos: internal fields of the fused stage pairs
     Coef coef;
     cudaStream_t own = nullptr, user = nullptr;
     DevBuf scratch[2];  // per precision: ya, yb, acc (x batch) for DoRK4 / Euler ping-pong
     int scratch_items[2] = {0, 0};
+    DevBuf wide;        // fused-pair fields (geometry g4): two step-start/accumulator fields and y2 (x batch)
+    int wide_items = 0;
     DevBuf err;         // device error word
     DevBuf red;         // reduction scratch (8 doubles)
     DevBuf dense;       // staging for the host-buffer entry point
@@ -126,6 +129,17 @@ struct sp_convection {
         sh.zchunk = std::max(1, zc);
         Tune t;
         t.set_all(sh);
+        // FP64 RK4: fused stage pairs, 8-row tiles, z-chunks for ~6 CTAs per SM
+        if (prec == 0 && pair_supported(g4)) {
+            const long long ptiles = (long long)((P.ni + 63) / 64) * ((P.nj + 7) / 8) * items;
+            int pz = P.nk;
+            while (pz > 16 && ptiles * ((P.nk + pz - 1) / pz) < 148LL * 6) pz = (pz + 1) / 2;
+            Shape ps;
+            ps.ty = 8;
+            ps.zchunk = pz;
+            t.pair[0] = t.pair[1] = ps;
+            t.fused = 1;
+        }
         return t;
     }
     void drop_graphs() {
@@ -141,6 +155,19 @@ struct sp_convection {
         if (e != cudaSuccess) return fail(SP_ERR_NOMEM, "scratch allocation of %zu bytes: %s", n, cudaGetErrorString(e));
         scratch_items[prec] = items;
         return SP_OK;
+    }
+    int ensure_wide(int items) {
+        if (wide_items >= items) return SP_OK;
+        drop_graphs();
+        const size_t n = (size_t)3 * items * g4.total * g4.es;
+        cudaError_t e = wide.alloc(n);
+        if (e != cudaSuccess) return fail(SP_ERR_NOMEM, "fused-pair fields of %zu bytes: %s", n, cudaGetErrorString(e));
+        wide_items = items;
+        return SP_OK;
+    }
+    // fused-pair field `which` (0, 1: step start / accumulator, 2: y2) of a batch of `items`
+    void* wbuf(int which, int items) const {
+        return static_cast<char*>(wide.p) + (size_t)which * items * g4.total * g4.es;
     }
     void* sbuf(int prec, int which, int items) const {
         return static_cast<char*>(scratch[prec].p) + (size_t)which * items * g[prec].total * g[prec].es;
@@ -250,6 +277,57 @@ int get_chunk_graph(sp_convection* h, int prec, void* field, double dt, double n
     return SP_OK;
 }
 
+// One fused RK4 step on internal fields (geometry g4): q -> (y2, acc) -> out,
+// where out is `acc` (geometry g4, updated in place) or a caller field of geometry go.
+cudaError_t enqueue_pair_step(sp_convection* h, const Tune& t, double dt, double nu, const void* q, void* acc,
+                              void* y2, void* out, const Geo& go, int items, const int* item_lo, int item_base,
+                              cudaStream_t s, int* err) {
+    PairLaunch L;
+    L.items = items;
+    L.item_lo = item_lo;
+    L.item_base = item_base;
+    L.nu = nu;
+    L.dt = dt;
+    L.coef = h->coef;
+    L.pair = 0; L.q = q; L.y2 = y2; L.acc = acc;
+    cudaError_t e = launch_pair(h->g4, h->g4, L, t.pair[0], s, err);
+    if (e != cudaSuccess) return e;
+    L.pair = 1; L.out = out;
+    return launch_pair(h->g4, go, L, t.pair[1], s, err);
+}
+
+// Graph of `n` (even) internal fused steps starting from wbuf(0) (constant nu, one field).
+int get_fused_graph(sp_convection* h, double dt, double nu, int n, GraphEntry** out) {
+    auto key = std::make_tuple(2, (const void*)nullptr, dt, nu, n);
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) { *out = &it->second; return SP_OK; }
+    if (h->graphs.size() > 32) h->drop_graphs();
+    const Tune t = h->tune(0, 1);
+    cudaStream_t s = h->stream();
+    SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    const long long before = launches();
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        void* Q = h->wbuf(i % 2, 1);
+        void* A = h->wbuf((i + 1) % 2, 1);
+        e = enqueue_pair_step(h, t, dt, nu, Q, A, h->wbuf(2, 1), A, h->g4, 1, nullptr, 0, s, h->err.as<int>());
+    }
+    const long long nodes = launches() - before;
+    add_launches(-nodes);  // captured, not launched
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return fail(SP_ERR_CUDA, "capture: %s", cudaGetErrorString(e)); }
+    if (e2 != cudaSuccess) return fail(SP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+    GraphEntry ge;
+    e = cudaGraphInstantiate(&ge.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    ge.nodes = nodes;
+    auto res = h->graphs.emplace(key, ge);
+    *out = &res.first->second;
+    return SP_OK;
+}
+
 bool capturing(cudaStream_t s) {
     cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &st);
@@ -273,7 +351,29 @@ int do_prop(sp_convection* h, int prec, bool rk, const void* in, void* out, doub
     // Periodicity on the input, in place, as before the reference's first stencil.
     SP_CUDA(launch_periodicity(g, const_cast<void*>(in), 1, s));
     const bool const_nu = h->P.nufreq == 0.;
-    if (rk) {
+    if (rk && t.fused && prec == 0 && pair_supported(h->g4)) {
+        // fused stage pairs: widen the input once, alternate the step-start
+        // field between wbuf(0) and wbuf(1), write the last step to `out`
+        if ((rc = h->ensure_wide(1))) return rc;
+        SP_CUDA(launch_widen(h->g4, h->wbuf(0, 1), g, in, 1, nullptr, 0, s));
+        int i = 0;
+        if (const_nu && !capturing(s) && n - 1 >= kChunk) {
+            GraphEntry* ge = nullptr;
+            if ((rc = get_fused_graph(h, dt, computenu(h->P.nu0, h->P.nufreq, tStart), kChunk, &ge))) return rc;
+            for (; n - 1 - i >= kChunk; i += kChunk) {  // kChunk is even: every chunk starts at wbuf(0)
+                SP_CUDA(cudaGraphLaunch(ge->exec, s));
+                add_launches(ge->nodes);
+            }
+        }
+        for (; i < n; ++i) {
+            const double tt = tStart + i * dt;  // Convection.cpp:302
+            void* Q = h->wbuf(i % 2, 1);
+            void* A = h->wbuf((i + 1) % 2, 1);
+            const bool last = i == n - 1;
+            SP_CUDA(enqueue_pair_step(h, t, dt, computenu(h->P.nu0, h->P.nufreq, tt), Q, A, h->wbuf(2, 1),
+                                      last ? out : A, last ? g : h->g4, 1, nullptr, 0, s, err));
+        }
+    } else if (rk) {
         SP_CUDA(enqueue_rk4_step(g, prec, h->coef, dt, NuSrc{computenu(h->P.nu0, h->P.nufreq, tStart), nullptr}, in,
                                  out, h->sbuf(prec, 0, 1), h->sbuf(prec, 1, 1), h->sbuf(prec, 2, 1), 1, nullptr, 0, t,
                                  s, err));
@@ -357,6 +457,7 @@ int sp_convection_create(const sp_params* p, int device, sp_convection** out) {
     h->device = device;
     h->g[0] = make_geo(p->ni, p->nj, p->nk, 8);
     h->g[1] = make_geo(p->ni, p->nj, p->nk, 4);
+    h->g4 = make_geo(p->ni, p->nj, p->nk, 8, 4);
     h->coef = make_coef(p->dx, p->cx, p->cy, p->cz, p->upwind);
     SP_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
     if (h->err.alloc(64) != cudaSuccess) return fail(SP_ERR_NOMEM, "error word");
@@ -396,28 +497,52 @@ int sp_convection_synchronize(sp_convection* h) {
 
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
-    if (ty != 4 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "ty must be 4, 8 or 16");
     if (zchunk < 1) return fail(SP_ERR_INVALID, "zchunk must be >= 1");
-    if (kind < 0 || kind > 1) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct) or 1 (TMA)");
+    if (kind < 0 || kind > 2) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA) or 2 (fused pairs)");
+    if (kind == 2) {
+        if (precision != SP_F64 || !pair_supported(h->g4))
+            return fail(SP_ERR_INVALID, "fused stage pairs need FP64 and at least 4 cells per axis");
+        if (ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "fused pairs: ty must be 8 or 16");
+        Tune t = h->tune(precision, batch);
+        Shape sh;
+        sh.ty = ty;
+        sh.zchunk = zchunk;
+        t.pair[0] = t.pair[1] = sh;
+        t.fused = 1;
+        h->tunes[{precision, batch}] = t;
+        h->drop_graphs();
+        return SP_OK;
+    }
+    if (ty != 4 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "ty must be 4, 8 or 16");
     Shape sh;
     sh.ty = ty;
     sh.zchunk = zchunk;
     sh.tma = kind;
     Tune t;
     t.set_all(sh);
+    t.fused = 0;
     h->tunes[{precision, batch}] = t;
-    for (auto& kv : h->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    h->graphs.clear();
+    h->drop_graphs();
     return SP_OK;
 }
 
+// op 0..8: single-stage kernels (tma: 0 direct, 1 TMA); op 9, 10: fused pairs
+// 1+2 and 3+4 (tma: 2 when RK4 steps run fused, else 0).
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* tma) {
     if (!h) return fail(SP_ERR_INVALID, "null handle");
-    const Shape t = h->tune(precision, batch).op[op < 0 || op >= kNumOps ? OP_RK_S2 : op];
+    const Tune tn = h->tune(precision, batch);
+    Shape t;
+    int kind;
+    if (op == kNumOps || op == kNumOps + 1) {
+        t = tn.pair[op - kNumOps];
+        kind = tn.fused ? 2 : 0;
+    } else {
+        t = tn.op[op < 0 || op >= kNumOps ? OP_RK_S2 : op];
+        kind = t.tma;
+    }
     if (ty) *ty = t.ty;
     if (zchunk) *zchunk = t.zchunk;
-    if (tma) *tma = t.tma;
+    if (tma) *tma = kind;
     return SP_OK;
 }
 
@@ -541,6 +666,8 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     Tune best = h->tune(precision, batch);
     std::vector<int> zcs = {4, 8, 16, 32, 64};
     zcs.push_back(g.nk);
+    float op_ms[kNumOps];
+    for (auto& m : op_ms) m = 1e30f;
     for (int op : {OP_RK_S1, OP_RK_S2, OP_RK_S3, OP_RK_S4, OP_EULER}) {
         StageLaunch L;
         L.op = op;
@@ -574,6 +701,50 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                     }
                     if (ms < best_ms) { best_ms = ms; best.op[op] = sh; }
                 }
+        op_ms[op] = best_ms;
+    }
+    // fused stage pairs (FP64): best shape per pair, then fused or single-stage
+    // steps by the sum of their kernel times
+    best.fused = 0;
+    if (precision == SP_F64 && pair_supported(h->g4)) {
+        const Geo& g4 = h->g4;
+        const size_t wb = (size_t)batch * g4.total * g4.es;
+        DevBuf wbuf;
+        if (wbuf.alloc(3 * wb) == cudaSuccess) {
+            char* w = wbuf.as<char>();
+            float pair_ms[2] = {1e30f, 1e30f};
+            for (int pair = 0; pair < 2; ++pair) {
+                PairLaunch L;
+                L.pair = pair;
+                L.items = batch;
+                L.coef = h->coef;
+                L.nu = h->P.nu0;
+                L.dt = 1e-9;
+                L.q = w; L.acc = w + wb; L.y2 = w + 2 * wb; L.out = w + wb;
+                for (int ty : {8, 16})
+                    for (int zc : {8, 12, 16, 24, 32, 48, 64, 128, g.nk}) {
+                        if (zc > g.nk) continue;
+                        if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
+                        Shape sh;
+                        sh.ty = ty; sh.zchunk = zc;
+                        cudaError_t e = launch_pair(g4, g4, L, sh, s, h->err.as<int>());
+                        if (e != cudaSuccess) { cudaGetLastError(); continue; }
+                        float ms = 1e30f;
+                        for (int r = 0; r < 3; ++r) {
+                            cudaEventRecord(e0, s);
+                            launch_pair(g4, g4, L, sh, s, h->err.as<int>());
+                            cudaEventRecord(e1, s);
+                            cudaEventSynchronize(e1);
+                            float m = 0;
+                            cudaEventElapsedTime(&m, e0, e1);
+                            ms = std::min(ms, m);
+                        }
+                        if (ms < pair_ms[pair]) { pair_ms[pair] = ms; best.pair[pair] = sh; }
+                    }
+            }
+            best.fused = (pair_ms[0] + pair_ms[1]) < (op_ms[OP_RK_S1] + op_ms[OP_RK_S2] + op_ms[OP_RK_S3] +
+                                                      op_ms[OP_RK_S4]) ? 1 : 0;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -1,0 +1,51 @@
+// sp_stencil.cuh -- the fourth-order right-hand side as 13 per-offset weights,
+// shared by the single-stage kernels (sp_kernels.cu) and the fused stage
+// pairs (sp_fused.cu), plus the tensor-map helper both use.
+#pragma once
+
+#include <cuda.h>
+
+#include "sp_device.cuh"
+#include "sp_internal.h"
+
+namespace sp {
+
+// R4 as 13 per-offset weights of the reference's coefficients
+// (RHS4 of src/Convection/Convection.cpp:40-112):
+//   ca_d (8(q[-1]-q[+1]) - (q[-2]-q[+2])) + nl (16 S1 - S2 - 90 q),  nl = nu/(12 dx^2).
+template <typename T>
+struct W13 {
+    T m1[3], p1[3], m2[3], p2[3], c;
+};
+
+template <typename T>
+inline void fill_w13(W13<T>& w, const Coef& c, double nu) {
+    const double nl = nu * c.s4;
+    for (int d = 0; d < 3; ++d) {
+        w.m1[d] = (T)(8. * c.ca[d] + 16. * nl);
+        w.p1[d] = (T)(-8. * c.ca[d] + 16. * nl);
+        w.m2[d] = (T)(-c.ca[d] - nl);
+        w.p2[d] = (T)(c.ca[d] - nl);
+    }
+    w.c = (T)(-90. * nl);
+}
+
+// The 13 stencil operands of one cell.
+template <typename T>
+struct Nb {
+    T c, xm1, xp1, xm2, xp2, ym1, yp1, ym2, yp2, zm1, zp1, zm2, zp2;
+};
+
+template <typename T>
+__device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
+    const T sx = fmaT(w.m2[0], s.xm2, fmaT(w.m1[0], s.xm1, fmaT(w.p1[0], s.xp1, w.p2[0] * s.xp2)));
+    const T sy = fmaT(w.m2[1], s.ym2, fmaT(w.m1[1], s.ym1, fmaT(w.p1[1], s.yp1, w.p2[1] * s.yp2)));
+    const T sz = fmaT(w.m2[2], s.zm2, fmaT(w.m1[2], s.zm1, fmaT(w.p1[2], s.zp1, w.p2[2] * s.zp2)));
+    return fmaT(w.c, s.c, (sx + sy) + sz);
+}
+
+// Tensor map over `items` fields of geometry g starting at `base`: dims
+// (px, py, pz*items), box (bw, bh, 1), no swizzle, out-of-range reads as zero.
+bool make_tmap(CUtensorMap* tm, const Geo& g, const void* base, int items, int bw, int bh);
+
+}  // namespace sp

@@ -62,10 +62,14 @@ class MatFile:
         return self.conv.download(field)
 
     def addField(self, name_or_field, field=None, inc: int = -1):
-        """addField(name, field[, inc]) at top level; addField(field, inc) inside a cell."""
+        """addField(name, field[, inc]), or addField(field[, inc]) under the name "q"
+        (the reference takes the field's own name, MatFile.h:171-174; the
+        reference drivers name their solution fields "q").  Inside a cell the
+        field becomes the next element and the name is not used."""
+        if not isinstance(name_or_field, str):  # addField(field[, inc]): inc is the 2nd argument
+            name_or_field, field, inc = "q", name_or_field, (inc if field is None else field)
         if self._cell is not None:
-            f = name_or_field if field is None else field
-            self._cell[1].append(_numeric("", self._dense(f)))
+            self._cell[1].append(_numeric("", self._dense(field)))
             return
         name = name_or_field if inc < 0 else f"{name_or_field}_{inc}"
         self.f.write(_numeric(name, self._dense(field)))

@@ -49,15 +49,17 @@ def test_matfile_roundtrip(tmp_path):
     with MatFile(fn) as m:
         m.addField("q", a)
         m.addField("q", a, inc=3)
+        m.addField(b, 2)  # addField(field, inc): the name "q" with _inc
         m.startCell("series", 2)
-        m.addField(a)
-        m.addField(b)
+        m.addField(a, 0)
+        m.addField(b, 1)
         m.endCell()
     d = scipy.io.loadmat(fn)
     # MATLAB q(i, j, k) = interior cell (i, j, k): dims ni x nj x nk, i fastest
     assert d["q"].shape == (6, 5, 4)
     np.testing.assert_array_equal(d["q"], a.transpose(2, 1, 0))
     np.testing.assert_array_equal(d["q_3"], a.transpose(2, 1, 0))
+    np.testing.assert_array_equal(d["q_2"], b.transpose(2, 1, 0))
     cell = d["series"]
     assert cell.shape == (1, 2)
     np.testing.assert_array_equal(cell[0, 1], b.transpose(2, 1, 0))
