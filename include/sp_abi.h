@@ -246,13 +246,18 @@ int sp_abi_version(void);
 long long sp_launch_count(void);
 /* Launch shape in use for a grid / batch and stage kernel `op` (0..3 = RK4 stages
  * S1..S4, 4 = Euler): tile rows ty, z-chunk, kernel kind (0 direct loads, 1
- * TMA/mbarrier pipeline). */
+ * TMA/mbarrier pipeline).  op 9 and 10: the fused stage pairs 1+2 and 3+4 of
+ * FP64 RK4 steps: tile rows, planes per CTA (0 = one range per resident CTA),
+ * kind 2 when RK4 steps run as fused pairs, else 0. */
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* kind);
 /* Runs the autotuner for this handle's grid at `batch` fields and precision: every
- * stage kernel gets the fastest of its candidate launch shapes. */
+ * stage kernel gets the fastest of its candidate launch shapes, and FP64 RK4
+ * steps run as fused pairs when those are faster than the four stages. */
 int sp_autotune(sp_convection* h, int precision, int batch);
-/* Forces one launch shape on every stage kernel for a precision and batch:
- * ty in {4,8,16}, zchunk >= 1, kind as in sp_tuned_config. */
+/* Forces one launch shape for a precision and batch.  kind 0 or 1: every
+ * single-stage kernel, ty in {4,8,16}, zchunk >= 1, RK4 steps unfused.  kind 2
+ * (FP64): RK4 steps as fused pairs with ty in {8,16} and zchunk planes per CTA
+ * (0 = automatic). */
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind);
 
 #ifdef __cplusplus

@@ -124,6 +124,22 @@ __device__ __forceinline__ void st16(T* p, const Vec<T, V16<T>::N>& r) {
     }
 }
 
+// 16-byte shared-memory access by 32-bit shared address (offset OFF bytes).
+__device__ __forceinline__ Vec<double, 2> lds2(uint32_t addr) {
+    Vec<double, 2> r;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(r.v[0]), "=d"(r.v[1]) : "r"(addr));
+    return r;
+}
+template <int OFF>
+__device__ __forceinline__ Vec<double, 2> lds2o(uint32_t addr) {
+    Vec<double, 2> r;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2+%3];" : "=d"(r.v[0]), "=d"(r.v[1]) : "r"(addr), "n"(OFF));
+    return r;
+}
+__device__ __forceinline__ void sts2(uint32_t addr, const Vec<double, 2>& v) {
+    asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.v[0]), "d"(v.v[1]) : "memory");
+}
+
 template <typename T>
 __device__ __forceinline__ T fmaT(T a, T b, T c) {
     if constexpr (sizeof(T) == 8) return fma(a, b, c);

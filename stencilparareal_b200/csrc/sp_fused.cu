@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "sp_device.cuh"
@@ -45,7 +46,8 @@ using V2 = Vec<double, 2>;
 struct PairArgs {
     long long item_stride, origin, px, plane;  // internal geometry (4-cell halo)
     int ni, nj, nk, pz;
-    int tiles_x, zchunk;
+    int tiles_x, tiles_y, items;
+    int span;          // planes of the flattened (tile, z) space per CTA (total < 2^31)
     const int* item_lo;
     int item_base;
     W13<double> w;
@@ -59,12 +61,8 @@ struct PairArgs {
     int* err;
 };
 
-// Stores cells (x, x+1) of row (y, z) and every periodic image of them that
-// lies within `hd` cells of a face (faces, edges and corners).  base: the
-// item's interior origin; x < ni.  The cell itself is one 16-byte store; the
-// x-images of the row are a short branch taken by the lanes at the x faces,
-// and the copies of the row into the y/z halo a longer one taken only on the
-// rows and planes next to those faces.
+// Stores cells (x, x+1) of a row and their x-images within `hd` cells of the
+// x faces; x < ni.
 __device__ __forceinline__ void row_pair(double* row, int ni, int hd, int x, const V2& v) {
     if (x + 2 <= ni) st16<double>(row + x, v);
     else row[x] = v.v[0];
@@ -79,36 +77,37 @@ __device__ __forceinline__ void row_pair(double* row, int ni, int hd, int x, con
     }
 }
 
-__device__ __forceinline__ void store_pair(double* base, long long px, long long plane, int ni, int nj, int nk,
-                                           int hd, int x, int y, int z, const V2& v) {
+// Stores cells (x, x+1) of row (y, z) (x < ni) and their periodic images
+// within `hd` cells of a face (faces, edges and corners): the path of the
+// lanes next to a face; the others store their pair with one 16-byte store.
+__device__ __forceinline__ void store_images_pair(double* base, long long px, long long plane, int ni, int nj,
+                                                  int nk, int hd, int x, int y, int z, const V2& v) {
     double* row = base + (long long)z * plane + (long long)y * px;
-    row_pair(row, ni, hd, x, v);
-    if (y < hd || y >= nj - hd || z < hd || z >= nk - hd) {
 #pragma unroll
-        for (int iz = 0; iz < 3; ++iz) {
-            if (iz == 1 && !(z < hd)) continue;
-            if (iz == 2 && !(z >= nk - hd)) continue;
-            const long long oz = iz == 0 ? 0 : (iz == 1 ? (long long)nk * plane : -(long long)nk * plane);
+    for (int iz = 0; iz < 3; ++iz) {
+        if (iz == 1 && !(z < hd)) continue;
+        if (iz == 2 && !(z >= nk - hd)) continue;
+        const long long oz = iz == 0 ? 0 : (iz == 1 ? (long long)nk * plane : -(long long)nk * plane);
 #pragma unroll
-            for (int iy = 0; iy < 3; ++iy) {
-                if (iz == 0 && iy == 0) continue;  // the row itself
-                if (iy == 1 && !(y < hd)) continue;
-                if (iy == 2 && !(y >= nj - hd)) continue;
-                const long long oy = iy == 0 ? 0 : (iy == 1 ? (long long)nj * px : -(long long)nj * px);
-                row_pair(row + oz + oy, ni, hd, x, v);
-            }
+        for (int iy = 0; iy < 3; ++iy) {
+            if (iy == 1 && !(y < hd)) continue;
+            if (iy == 2 && !(y >= nj - hd)) continue;
+            const long long oy = iy == 0 ? 0 : (iy == 1 ? (long long)nj * px : -(long long)nj * px);
+            double* r = row + oz + oy;
+            row_pair(r, ni, hd, x, v);
         }
     }
 }
 
-// R4 of cells (pos, pos+1) of a slot of row width W; the centre values and
-// the z-neighbours are given, the x- and y-neighbours are read from the slot.
+// R4 of cells (at, at+8) of a slot of row width W, `at` a shared-memory byte
+// address; the centre values and the z-neighbours are given, the x- and
+// y-neighbours are read from the slot.
 template <int W>
-__device__ __forceinline__ void rhs_c(const W13<double>& wt, const double* C, int pos, const V2& cen,
-                                      const V2& zm2, const V2& zm1, const V2& zp1, const V2& zp2, double k[2]) {
-    const V2 r0 = ld16<double>(C + pos - 2), r2 = ld16<double>(C + pos + 2);
-    const V2 ym2 = ld16<double>(C + pos - 2 * W), ym1 = ld16<double>(C + pos - W);
-    const V2 yp1 = ld16<double>(C + pos + W), yp2 = ld16<double>(C + pos + 2 * W);
+__device__ __forceinline__ void rhs_s(const W13<double>& wt, uint32_t at, const V2& cen, const V2& zm2,
+                                      const V2& zm1, const V2& zp1, const V2& zp2, double k[2]) {
+    const V2 r0 = lds2o<-16>(at), r2 = lds2o<16>(at);
+    const V2 ym2 = lds2o<-16 * W>(at), ym1 = lds2o<-8 * W>(at);
+    const V2 yp1 = lds2o<8 * W>(at), yp2 = lds2o<16 * W>(at);
     const double row[6] = {r0.v[0], r0.v[1], cen.v[0], cen.v[1], r2.v[0], r2.v[1]};
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -153,15 +152,6 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     double* ps = es + NE * SE;
     uint64_t* bar = reinterpret_cast<uint64_t*>(ps + NP * SP);
 
-    const int b = blockIdx.z;
-    if (a.item_lo && b + a.item_base < *a.item_lo) return;
-    const int x0 = (blockIdx.x % a.tiles_x) * TX;
-    const int y0 = (blockIdx.x / a.tiles_x) * TY;
-    const int z0 = blockIdx.y * a.zchunk;
-    const int z1 = min(z0 + a.zchunk, a.nk);
-    const int nv = z1 - z0 + 4;  // first-stage planes z0-2 .. z1+1
-    const int nu = z1 - z0 + 8;  // stencil planes z0-4 .. z1+3
-    const int zs = b * a.pz + z0;  // tensor-map plane of stencil plane 0 (interior z0-4)
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const bool leader = tid == 0;
 
@@ -173,35 +163,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     }
     __syncthreads();
 
-    // stencil plane u -> slot u % NSQ; pointwise plane v -> slot v % NP
-    auto issue_s = [&](int u) {
-        const int s = u % NSQ;
-        mbar_arrive_expect_tx(&bar[s], SBYTES);
-        tma_load_3d(sb + s * SB, &tm_s, x0, y0, zs + u, &bar[s]);  // interior (x0-4, y0-4)
-    };
-    auto issue_p = [&](int v) {
-        const int s = v % NP;
-        mbar_arrive_expect_tx(&bar[NSQ + s], PBYTES);
-        double* d = ps + s * SP;
-        tma_load_3d(d, &tm_q, x0 + 2, y0 + 2, zs + 2 + v, &bar[NSQ + s]);       // q, interior (x0-2, y0-2)
-        tma_load_3d(d + SE, &tm_a, x0 + 4, y0 + 4, zs + 2 + v, &bar[NSQ + s]);  // acc, interior (x0, y0)
-    };
-    int s_hi = -1, p_hi = -1;  // highest planes issued (leader)
-    if (leader) {
-        for (int u = 0; u < NSQ && u < nu; ++u) { issue_s(u); s_hi = u; }
-        if constexpr (PAIR == 1)
-            for (int v = 0; v < NP && v < nv; ++v) { issue_p(v); p_hi = v; }
-    }
-    auto drain = [&](int s_done, int p_done) {
-        if (!leader) return;
-        for (int u = s_done + 1; u <= s_hi; ++u) (void)mbar_wait_bounded(&bar[u % NSQ], (uint32_t)((u / NSQ) & 1));
-        for (int v = p_done + 1; v <= p_hi; ++v)
-            (void)mbar_wait_bounded(&bar[NSQ + v % NP], (uint32_t)((v / NP) & 1));
-    };
-
     // own cells and ring chunk
-    const int m_s = (w + 4) * WB + 2 * lane + 4;
-    const int m_e = (w + 2) * WE + 2 * lane + 2;
     const bool has_h = tid < NH;
     // the ring: rows y0-2, y0-1, y0+TY, y0+TY+1 over the tile's columns, and
     // columns x0-2..x0-1, x0+64..x0+65 over the tile's rows (the corners are
@@ -216,160 +178,236 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
         hey = 2 + (d >> 1);
         hex = (d & 1) ? WE - 2 : 0;
     }
-    const int h_s = (hey + 2) * WB + hex + 2;
-    const int h_e = hey * WE + hex;
+    // byte offsets in the slots
+    const uint32_t m_s8 = ((w + 4) * WB + 2 * lane + 4) * 8;
+    const uint32_t m_e8 = ((w + 2) * WE + 2 * lane + 2) * 8;
+    [[maybe_unused]] const uint32_t m_a8 = (w * TX + 2 * lane) * 8;
+    const uint32_t h_s8 = ((hey + 2) * WB + hex + 2) * 8;
+    const uint32_t h_e8 = (hey * WE + hex) * 8;
+    constexpr uint32_t EBYTES = SE * 8;
+    [[maybe_unused]] constexpr uint32_t SEBYTES = SE * 8;
+    const uint32_t s_base = smem_u32(sb), e_base = smem_u32(es);
+    [[maybe_unused]] const uint32_t p_base = smem_u32(ps);
 
-    bool bad = false;
-    // Register windows of the own cells, indexed by plane mod 5 so that the
-    // loop, unrolled by 5, renames registers instead of moving them:
-    //   qw[u % 5]: stencil input at stencil plane u (planes v .. v+4 live)
-    //   ew[p % 5]: first-stage value at first-stage plane p (p = v-4 .. v)
-    //   aw[p % 5]: first-stage accumulator partial (p = v-2 .. v)
-    V2 qw[5], ew[5], aw[5];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {  // prologue: stencil planes 0..3
-        if (!mbar_wait_bounded(&bar[u], 0)) bad = true;
-        qw[u] = ld16<double>(sb + u * SB + m_s);
-    }
-#pragma unroll
-    for (int u = 0; u < 5; ++u) ew[u] = aw[u] = V2{};
+    // This CTA's planes: [g_lo, g_hi) of all (tile, z) planes, tiles ordered x
+    // fastest, then y, then item.  A segment is the part inside one tile; each
+    // segment pays 4 extra plane iterations to fill the pipeline.
+    const int tiles_xy = a.tiles_x * a.tiles_y;
+    const int total = tiles_xy * a.items * a.nk;
+    const int g_lo = blockIdx.x * a.span;
+    const int g_hi = min(g_lo + a.span, total);
+    unsigned U = 0, VP = 0;  // stencil / pointwise planes this CTA has loaded: ring positions
+    for (int g = g_lo; g < g_hi;) {
+        const int tile = g / a.nk;
+        const int z0 = g - tile * a.nk;
+        const int z1 = min(a.nk, z0 + (g_hi - g));
+        g += z1 - z0;
+        const int b = tile / tiles_xy;
+        const int txy = tile - b * tiles_xy;
+        if (a.item_lo && b + a.item_base < *a.item_lo) continue;  // the same for all threads
+        const int x0 = (txy % a.tiles_x) * TX;
+        const int y0 = (txy / a.tiles_x) * TY;
+        const int nv = z1 - z0 + 4;      // first-stage planes z0-2 .. z1+1
+        const int nu = z1 - z0 + 8;      // stencil planes z0-4 .. z1+3
+        const int zs = b * a.pz + z0;    // tensor-map plane of stencil plane 0 (interior z0-4)
 
-    const int x = x0 + 2 * lane;
-    const int y = y0 + w;
-    const bool live = x < a.ni && y < a.nj;
-    const long long ob = (long long)b * a.item_stride + a.origin;
-    double* const ybase = a.yout ? a.yout + ob : nullptr;
-    double* arow = nullptr;
-    if constexpr (PAIR == 0) arow = a.aout + ob + (long long)(z0 - 4) * a.plane + (long long)y * a.px + x;
-    double* const obase = PAIR == 1 ? a.qout + (long long)b * a.o_item_stride + a.o_origin : nullptr;
-
-    int s_v = 0;                    // slot of stencil plane v
-    int s_4 = 4 % NSQ;              // slot and phase of stencil plane v+4
-    uint32_t ph_4 = (4 / NSQ) & 1;
-    int e_v = 0;                    // slot of first-stage plane v (mod 3)
-    int sp_v = 0;                   // pointwise slot and phase of plane v
-    uint32_t ph_p = 0;
-
-    // One plane iteration; K = v mod 5.  Returns false when the CTA must stop.
-    auto iterate = [&](auto kc, int v) -> bool {
-        constexpr int K = decltype(kc)::value;
-        if (!mbar_wait_bounded(&bar[s_4], ph_4)) bad = true;
-        auto slot = [&](int k) {
-            int s = s_v + k;
-            if (s >= NSQ) s -= NSQ;
-            return sb + s * SB;
+        // stencil plane u -> ring position U+u; pointwise plane v -> VP+v
+        auto issue_s = [&](int u) {
+            const int s = (int)((U + u) % NSQ);
+            mbar_arrive_expect_tx(&bar[s], SBYTES);
+            tma_load_3d(sb + s * SB, &tm_s, x0, y0, zs + u, &bar[s]);  // interior (x0-4, y0-4)
         };
-        const double* P0 = slot(0);
-        const double* P1 = slot(1);
-        const double* P2 = slot(2);
-        const double* P3 = slot(3);
-        const double* P4 = slot(4);
-        qw[(K + 4) % 5] = ld16<double>(P4 + m_s);
-        const double* PW = nullptr;
-        if constexpr (PAIR == 1) {
-            if (!mbar_wait_bounded(&bar[NSQ + sp_v], ph_p)) bad = true;
-            PW = ps + sp_v * SP;
-        }
-        double* E = es + e_v * SE;
-        (void)PW;
-
-        // first stage, own cells (first-stage plane v, stencil centre v+2;
-        // the centre value is the window's)
-        {
-            double k[2];
-            rhs_c<WB>(a.w, P2, m_s, qw[(K + 2) % 5], qw[K], qw[(K + 1) % 5], qw[(K + 3) % 5], qw[(K + 4) % 5], k);
-            V2 en, an;
-            if constexpr (PAIR == 0) {
-                const V2& c = qw[(K + 2) % 5];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    en.v[e] = fmaT(a.c1y, k[e], c.v[e]);
-                    an.v[e] = fmaT(a.c1a, k[e], c.v[e]);
-                }
-            } else {
-                const V2 qv = ld16<double>(PW + m_e);
-                const V2 av = ld16<double>(PW + SE + w * TX + 2 * lane);
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    en.v[e] = fmaT(a.c1y, k[e], qv.v[e]);
-                    an.v[e] = fmaT(a.c1a, k[e], av.v[e]);
-                }
-            }
-            st16<double>(E + m_e, en);
-            ew[K] = en;
-            aw[K] = an;
-        }
-        // first stage, ring chunk
-        if (has_h) {
-            const V2 zm2 = ld16<double>(P0 + h_s), zm1 = ld16<double>(P1 + h_s);
-            const V2 zp1 = ld16<double>(P3 + h_s), zp2 = ld16<double>(P4 + h_s);
-            const V2 cen = ld16<double>(P2 + h_s);
-            V2 hv;
-            double k[2];
-            rhs_c<WB>(a.w, P2, h_s, cen, zm2, zm1, zp1, zp2, k);
-            V2 base = cen;
-            if constexpr (PAIR == 1) base = ld16<double>(PW + h_e);
-#pragma unroll
-            for (int e = 0; e < 2; ++e) hv.v[e] = fmaT(a.c1y, k[e], base.v[e]);
-            st16<double>(E + h_e, hv);
-        }
-        // second stage on plane z0-4+v (first-stage plane v-2, stencil plane v)
-        if (v >= 4) {
-            const int ez = e_v == 2 ? 0 : e_v + 1;  // slot of first-stage plane v-2
-            double k[2];
-            rhs_c<WE>(a.w, es + ez * SE, m_e, ew[(K + 3) % 5], ew[(K + 1) % 5], ew[(K + 2) % 5], ew[(K + 4) % 5],
-                      ew[K], k);
-            const V2& ap = aw[(K + 3) % 5];
-            V2 o;
-            [[maybe_unused]] V2 oa;
-            if constexpr (PAIR == 0) {
-                const V2& qc = qw[K];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    o.v[e] = fmaT(a.c2y, k[e], qc.v[e]);
-                    oa.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
-                }
-            } else {
-#pragma unroll
-                for (int e = 0; e < 2; ++e) o.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
-            }
-            if (live) {
-                const int z = z0 - 4 + v;
-                if constexpr (PAIR == 0) {
-                    store_pair(ybase, a.px, a.plane, a.ni, a.nj, a.nk, 4, x, y, z, o);
-                    if (x + 2 <= a.ni) st16<double>(arow, oa);
-                    else arow[0] = oa.v[0];
-                } else {
-                    store_pair(obase, a.o_px, a.o_plane, a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
-                }
-            }
-        }
-        if constexpr (PAIR == 0) arow += a.plane;  // plane z0-4+v -> next
-        if (__syncthreads_or(bad)) {
-            if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
-            drain(v + 4, v);
-            return false;
-        }
+        auto issue_p = [&](int v) {
+            const int s = (int)((VP + v) % NP);
+            mbar_arrive_expect_tx(&bar[NSQ + s], PBYTES);
+            double* d = ps + s * SP;
+            tma_load_3d(d, &tm_q, x0 + 2, y0 + 2, zs + 2 + v, &bar[NSQ + s]);       // q, interior (x0-2, y0-2)
+            tma_load_3d(d + SE, &tm_a, x0 + 4, y0 + 4, zs + 2 + v, &bar[NSQ + s]);  // acc, interior (x0, y0)
+        };
+        int s_hi = -1, p_hi = -1;  // highest planes issued (leader)
         if (leader) {
-            fence_proxy_async_smem();
-            if (v + NSQ < nu) { issue_s(v + NSQ); s_hi = v + NSQ; }
+            fence_proxy_async_smem();  // the slots were last read by the previous segment
+            for (int u = 0; u < NSQ && u < nu; ++u) { issue_s(u); s_hi = u; }
             if constexpr (PAIR == 1)
-                if (v + NP < nv) { issue_p(v + NP); p_hi = v + NP; }
+                for (int v = 0; v < NP && v < nv; ++v) { issue_p(v); p_hi = v; }
         }
-        if (++s_v == NSQ) s_v = 0;
-        if (++s_4 == NSQ) { s_4 = 0; ph_4 ^= 1u; }
-        if (++e_v == 3) e_v = 0;
-        if constexpr (PAIR == 1)
-            if (++sp_v == NP) { sp_v = 0; ph_p ^= 1u; }
-        return true;
-    };
+        auto drain = [&](int s_done, int p_done) {
+            if (!leader) return;
+            for (int u = s_done + 1; u <= s_hi; ++u)
+                (void)mbar_wait_bounded(&bar[(U + u) % NSQ], (uint32_t)(((U + u) / NSQ) & 1));
+            for (int v = p_done + 1; v <= p_hi; ++v)
+                (void)mbar_wait_bounded(&bar[NSQ + (VP + v) % NP], (uint32_t)(((VP + v) / NP) & 1));
+        };
 
-    for (int vb = 0; vb < nv; vb += 5) {  // nv is uniform over the CTA
-        if (!iterate(std::integral_constant<int, 0>{}, vb)) return;
-        if (vb + 1 < nv && !iterate(std::integral_constant<int, 1>{}, vb + 1)) return;
-        if (vb + 2 < nv && !iterate(std::integral_constant<int, 2>{}, vb + 2)) return;
-        if (vb + 3 < nv && !iterate(std::integral_constant<int, 3>{}, vb + 3)) return;
-        if (vb + 4 < nv && !iterate(std::integral_constant<int, 4>{}, vb + 4)) return;
+        bool bad = false;
+        // Register windows of the own cells, indexed by plane mod 5 so that the
+        // loop, unrolled by 5, renames registers instead of moving them:
+        //   qw[u % 5]: stencil input at stencil plane u (planes v .. v+4 live)
+        //   ew[p % 5]: first-stage value at first-stage plane p (p = v-4 .. v)
+        //   aw[p % 5]: first-stage accumulator partial (p = v-2 .. v)
+        //   sa[u % 5]: shared address of the slot of stencil plane u
+        V2 qw[5], ew[5], aw[5];
+        uint32_t sa[5];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {  // prologue: stencil planes 0..3
+            const unsigned gu = U + u;
+            if (!mbar_wait_bounded(&bar[gu % NSQ], (gu / NSQ) & 1)) bad = true;
+            sa[u] = s_base + (gu % NSQ) * SBYTES;
+            qw[u] = lds2(sa[u] + m_s8);
+        }
+        sa[4] = 0;
+#pragma unroll
+        for (int u = 0; u < 5; ++u) ew[u] = aw[u] = V2{};
+
+        const int x = x0 + 2 * lane;
+        const int y = y0 + w;
+        const bool live = x < a.ni && y < a.nj;
+        const bool full = x + 2 <= a.ni;
+        // whether the cells have periodic images in x or y (image depth hd)
+        const int hd = PAIR == 0 ? 4 : a.o_halo;
+        const bool xy_img = x < hd || x + 2 > a.ni - hd || y < hd || y >= a.nj - hd || !full;
+        // the own cells' output columns at plane z0-4 (one plane further per iteration)
+        double* ocol;
+        [[maybe_unused]] double* acol = nullptr;
+        if constexpr (PAIR == 0) {
+            const long long ob = (long long)b * a.item_stride + a.origin + (long long)(z0 - 4) * a.plane +
+                                 (long long)y * a.px + x;
+            ocol = a.yout + ob;
+            acol = a.aout + ob;
+        } else {
+            ocol = a.qout + (long long)b * a.o_item_stride + a.o_origin + (long long)(z0 - 4) * a.o_plane +
+                   (long long)y * a.o_px + x;
+        }
+
+        int s_4 = (int)((U + 4) % NSQ);             // slot and phase of stencil plane v+4
+        uint32_t ph_4 = ((U + 4) / NSQ) & 1;
+        uint32_t e_cur = e_base;                    // first-stage slot of plane v (3 slots)
+        int sp_v = (int)(VP % NP);                  // pointwise slot and phase of plane v
+        uint32_t ph_p = (VP / NP) & 1;
+
+        // One plane iteration; K = v mod 5.  Returns false when the CTA must stop.
+        auto iterate = [&](auto kc, int v) -> bool {
+            constexpr int K = decltype(kc)::value;
+            if (!mbar_wait_bounded(&bar[s_4], ph_4)) bad = true;
+            sa[(K + 4) % 5] = s_base + s_4 * SBYTES;
+            const uint32_t S0 = sa[K], S1 = sa[(K + 1) % 5], S2 = sa[(K + 2) % 5], S3 = sa[(K + 3) % 5],
+                           S4 = sa[(K + 4) % 5];
+            qw[(K + 4) % 5] = lds2(S4 + m_s8);
+            [[maybe_unused]] uint32_t PW = 0;
+            if constexpr (PAIR == 1) {
+                if (!mbar_wait_bounded(&bar[NSQ + sp_v], ph_p)) bad = true;
+                PW = p_base + sp_v * PBYTES;
+            }
+            const uint32_t E = e_cur;
+            const uint32_t E2 = E == e_base + 2 * EBYTES ? e_base : E + EBYTES;  // slot of first-stage plane v-2
+
+            // first stage, own cells (first-stage plane v, stencil centre v+2;
+            // the centre value is the window's)
+            {
+                double k[2];
+                rhs_s<WB>(a.w, S2 + m_s8, qw[(K + 2) % 5], qw[K], qw[(K + 1) % 5], qw[(K + 3) % 5], qw[(K + 4) % 5], k);
+                V2 en, an;
+                if constexpr (PAIR == 0) {
+                    const V2& c = qw[(K + 2) % 5];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        en.v[e] = fmaT(a.c1y, k[e], c.v[e]);
+                        an.v[e] = fmaT(a.c1a, k[e], c.v[e]);
+                    }
+                } else {
+                    const V2 qv = lds2(PW + m_e8);
+                    const V2 av = lds2(PW + SEBYTES + m_a8);
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        en.v[e] = fmaT(a.c1y, k[e], qv.v[e]);
+                        an.v[e] = fmaT(a.c1a, k[e], av.v[e]);
+                    }
+                }
+                sts2(E + m_e8, en);
+                ew[K] = en;
+                aw[K] = an;
+            }
+            // first stage, ring chunk
+            if (has_h) {
+                const V2 zm2 = lds2(S0 + h_s8), zm1 = lds2(S1 + h_s8);
+                const V2 zp1 = lds2(S3 + h_s8), zp2 = lds2(S4 + h_s8);
+                const V2 cen = lds2(S2 + h_s8);
+                double k[2];
+                rhs_s<WB>(a.w, S2 + h_s8, cen, zm2, zm1, zp1, zp2, k);
+                V2 base = cen, hv;
+                if constexpr (PAIR == 1) base = lds2(PW + h_e8);
+#pragma unroll
+                for (int e = 0; e < 2; ++e) hv.v[e] = fmaT(a.c1y, k[e], base.v[e]);
+                sts2(E + h_e8, hv);
+            }
+            // second stage on plane z0-4+v (first-stage plane v-2, stencil plane v)
+            if (v >= 4) {
+                double k[2];
+                rhs_s<WE>(a.w, E2 + m_e8, ew[(K + 3) % 5], ew[(K + 1) % 5], ew[(K + 2) % 5], ew[(K + 4) % 5], ew[K], k);
+                const V2& ap = aw[(K + 3) % 5];
+                V2 o;
+                [[maybe_unused]] V2 oa;
+                if constexpr (PAIR == 0) {
+                    const V2& qc = qw[K];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        o.v[e] = fmaT(a.c2y, k[e], qc.v[e]);
+                        oa.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) o.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
+                }
+                if (live) {
+                    const int z = z0 - 4 + v;
+                    const bool inner = !xy_img && z >= hd && z < a.nk - hd;
+                    if constexpr (PAIR == 0) {
+                        if (inner)
+                            st16<double>(ocol, o);
+                        else
+                            store_images_pair(a.yout + (long long)b * a.item_stride + a.origin, a.px, a.plane, a.ni,
+                                              a.nj, a.nk, 4, x, y, z, o);
+                        if (full) st16<double>(acol, oa);
+                        else acol[0] = oa.v[0];
+                    } else {
+                        if (inner)
+                            st16<double>(ocol, o);
+                        else
+                            store_images_pair(a.qout + (long long)b * a.o_item_stride + a.o_origin, a.o_px,
+                                              a.o_plane, a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
+                    }
+                }
+            }
+            ocol += PAIR == 0 ? a.plane : a.o_plane;
+            if constexpr (PAIR == 0) acol += a.plane;
+            if (__syncthreads_or(bad)) {
+                if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+                drain(v + 4, v);
+                return false;
+            }
+            if (leader) {
+                fence_proxy_async_smem();
+                if (v + NSQ < nu) { issue_s(v + NSQ); s_hi = v + NSQ; }
+                if constexpr (PAIR == 1)
+                    if (v + NP < nv) { issue_p(v + NP); p_hi = v + NP; }
+            }
+            if (++s_4 == NSQ) { s_4 = 0; ph_4 ^= 1u; }
+            e_cur = E == e_base + 2 * EBYTES ? e_base : E + EBYTES;
+            if constexpr (PAIR == 1)
+                if (++sp_v == NP) { sp_v = 0; ph_p ^= 1u; }
+            return true;
+        };
+
+        for (int vb = 0; vb < nv; vb += 5) {  // nv is uniform over the CTA
+            if (!iterate(std::integral_constant<int, 0>{}, vb)) return;
+            if (vb + 1 < nv && !iterate(std::integral_constant<int, 1>{}, vb + 1)) return;
+            if (vb + 2 < nv && !iterate(std::integral_constant<int, 2>{}, vb + 2)) return;
+            if (vb + 3 < nv && !iterate(std::integral_constant<int, 3>{}, vb + 3)) return;
+            if (vb + 4 < nv && !iterate(std::integral_constant<int, 4>{}, vb + 4)) return;
+        }
+
+        U += nu;
+        if constexpr (PAIR == 1) VP += nv;
     }
 }
 
@@ -424,9 +462,20 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     a.item_stride = g4.total; a.origin = g4.origin; a.px = g4.px; a.plane = g4.plane;
     a.ni = g4.ni; a.nj = g4.nj; a.nk = g4.nk; a.pz = (int)g4.pz;
     a.tiles_x = (g4.ni + S::TX - 1) / S::TX;
-    const int tiles_y = (g4.nj + TY - 1) / TY;
-    a.zchunk = sh.zchunk;
-    const int nzc = (g4.nk + sh.zchunk - 1) / sh.zchunk;
+    a.tiles_y = (g4.nj + TY - 1) / TY;
+    a.items = L.items;
+    const long long total = (long long)a.tiles_x * a.tiles_y * L.items * g4.nk;
+    if (total >= 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    if (sh.zchunk > 0) {
+        a.span = sh.zchunk;
+    } else {  // persistent: one range per resident CTA
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP>, 32 * TY, S::smem);
+        const long long ctas = (long long)std::max(1, sms) * std::max(1, occ);
+        a.span = (int)std::max(1LL, (total + ctas - 1) / ctas);
+    }
     a.item_lo = L.item_lo;
     a.item_base = L.item_base;
     fill_w13<double>(a.w, L.coef, L.nu);
@@ -442,8 +491,9 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
         a.o_halo = go.halo;
     }
     a.err = err;
-    dim3 grid(a.tiles_x * tiles_y, nzc, L.items);
-    if (grid.y > 65535u || grid.z > 65535u) return cudaErrorInvalidConfiguration;
+    const long long nct = (total + a.span - 1) / a.span;
+    if (nct > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    const dim3 grid((unsigned)nct);
     k_rk4_pair<PAIR, TY, NSQ, NP><<<grid, 32 * TY, S::smem, s>>>(ts, tq, ta, a);
     return cudaGetLastError();
 }
@@ -474,7 +524,7 @@ cudaError_t prepare_pairs() {
 cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const Shape& sh, cudaStream_t s,
                         int* err) {
     add_launches(1);
-    if (!pair_supported(g4) || g4.halo != 4 || sh.zchunk < 1) return cudaErrorInvalidValue;
+    if (!pair_supported(g4) || g4.halo != 4 || sh.zchunk < 0) return cudaErrorInvalidValue;
     if (L.pair == 0) {
         if (sh.ty == 8) return launch_pair_T<0, 8, 7, 2>(g4, go, L, sh, s, err);
         if (sh.ty == 16) return launch_pair_T<0, 16, 7, 2>(g4, go, L, sh, s, err);

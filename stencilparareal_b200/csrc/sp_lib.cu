@@ -129,14 +129,11 @@ struct sp_convection {
         sh.zchunk = std::max(1, zc);
         Tune t;
         t.set_all(sh);
-        // FP64 RK4: fused stage pairs, 8-row tiles, z-chunks for ~6 CTAs per SM
+        // FP64 RK4: fused stage pairs, 8-row tiles, one plane range per resident CTA
         if (prec == 0 && pair_supported(g4)) {
-            const long long ptiles = (long long)((P.ni + 63) / 64) * ((P.nj + 7) / 8) * items;
-            int pz = P.nk;
-            while (pz > 16 && ptiles * ((P.nk + pz - 1) / pz) < 148LL * 6) pz = (pz + 1) / 2;
             Shape ps;
             ps.ty = 8;
-            ps.zchunk = pz;
+            ps.zchunk = 0;
             t.pair[0] = t.pair[1] = ps;
             t.fused = 1;
         }
@@ -497,8 +494,9 @@ int sp_convection_synchronize(sp_convection* h) {
 
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
-    if (zchunk < 1) return fail(SP_ERR_INVALID, "zchunk must be >= 1");
     if (kind < 0 || kind > 2) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA) or 2 (fused pairs)");
+    if (zchunk < (kind == 2 ? 0 : 1))
+        return fail(SP_ERR_INVALID, "zchunk must be >= 1 (>= 0 for fused pairs: planes per CTA, 0 = automatic)");
     if (kind == 2) {
         if (precision != SP_F64 || !pair_supported(h->g4))
             return fail(SP_ERR_INVALID, "fused stage pairs need FP64 and at least 4 cells per axis");
@@ -722,9 +720,8 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 L.dt = 1e-9;
                 L.q = w; L.acc = w + wb; L.y2 = w + 2 * wb; L.out = w + wb;
                 for (int ty : {8, 16})
-                    for (int zc : {8, 12, 16, 24, 32, 48, 64, 128, g.nk}) {
+                    for (int zc : {0, 16, 24, 32, 48, 64}) {
                         if (zc > g.nk) continue;
-                        if ((long long)((g.nk + zc - 1) / zc) > 65535) continue;
                         Shape sh;
                         sh.ty = ty; sh.zchunk = zc;
                         cudaError_t e = launch_pair(g4, g4, L, sh, s, h->err.as<int>());
