@@ -45,7 +45,13 @@ STEPS_PER_RUN = 500
 DT = 5e-5
 NU = 1e-3
 C = (1.0, 0.5, 0.25)
-BYTES_PER_CELL_UPDATE = 128  # 16 FP64 field accesses per RK4 step (4 fused stage kernels)
+# Algorithmic HBM bytes per cell of each kernel of an RK4 step (FP64 field
+# accesses x 8 B): fused pairs 1+2 (q -> y2, acc) and 3+4 (y2, q, acc -> q'),
+# or the four single-stage kernels.
+KERNEL_BYTES = {"P12": 24, "P34": 32, "S1": 24, "S2": 40, "S3": 40, "S4": 24}
+KERNEL_NAMES = {"P12": "k_rk4_pair<0,...> (RK4 stages 1+2)", "P34": "k_rk4_pair<1,...> (RK4 stages 3+4)",
+                "S1": "k_stage_tma<double,0,...>", "S2": "k_stage_tma<double,1,...>",
+                "S3": "k_stage_tma<double,2,...>", "S4": "k_stage_tma<double,3,...>"}
 WORKLOAD = (f"fine RK4 FP64 {N_FINE}^3 x {STEPS_PER_RUN} steps, c=(1,0.5,0.25), nu=1e-3, dt=5e-5, "
             "8-mode Fourier IC seed 1")
 
@@ -391,15 +397,20 @@ def main():
     e2e = cells * world / t_e2e / 1e9
 
     peak, peak_kind = peaks()
-    # the four stage kernels of an RK4 step are the whole timed region: per launch,
-    # 32 B x cells on average (128 B per cell-update) over the average launch time
-    achieved = BYTES_PER_CELL_UPDATE * n ** 3 * STEPS_PER_RUN * args.steps / t_local / 1e9
+    # roofline of the dominant kernel: its algorithmic bytes per launch over its
+    # average launch time, every kernel of a step timed with CUDA events on the
+    # library's stream
+    ktimes = conv.kernel_times(fin, DT, reps=20)
+    dom = max(ktimes, key=ktimes.get)
+    alg_launch = KERNEL_BYTES[dom] * n ** 3
+    achieved = alg_launch / (ktimes[dom] * 1e-3) / 1e9
+    step_bytes = sum(KERNEL_BYTES[k] for k in ktimes)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                traffic = json.load(f).get("bytes_per_launch_avg")
+                traffic = json.load(f).get("dram_bytes_per_launch", {}).get(dom)
         except Exception:
             traffic = None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -407,11 +418,12 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (each 256^3 FP64 field is 134 MB)",
                        "parallelism": f"replicas x{world}", "tune": tune},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "traffic_unit": "bytes per stage-kernel launch (ncu, profiles/)",
-                         "algorithmic_bytes_per_launch": BYTES_PER_CELL_UPDATE * n ** 3 / 4,
-                         "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "traffic_unit": "dram bytes per launch (ncu, profiles/traffic.json)",
+                         "algorithmic_bytes_per_launch": alg_launch, "kernel_ms": ktimes[dom],
+                         "kernel_times_ms": ktimes, "algorithmic_bytes_per_cell_update": step_bytes,
+                         "step_achieved_gbs": step_bytes * n ** 3 * STEPS_PER_RUN * args.steps / t_local / 1e9},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8)},
             "gpu_launches": int(launches), "clocks": clk.summary()}

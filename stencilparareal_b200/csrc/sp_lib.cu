@@ -644,6 +644,86 @@ int sp_field_errors(sp_convection* h, const double* a, const double* b, double* 
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Per-kernel durations of FP64 RK4 steps (CUDA events around every launch on
+// the handle's stream), on a copy of `field`; the field is not modified.
+extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, float* ms, int* count) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!field || !ms || !count || reps < 1) return fail(SP_ERR_INVALID, "bad arguments");
+    cudaStream_t s = h->stream();
+    if (capturing(s)) return fail(SP_ERR_STATE, "cannot time kernels while the stream is capturing");
+    const Tune t = h->tune(0, 1);
+    const Geo& g = h->g[0];
+    const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
+    int* err = h->err.as<int>();
+    float acc[4] = {0, 0, 0, 0};
+    const bool fused = t.fused && pair_supported(h->g4);
+    if (fused) {
+        if ((rc = h->ensure_wide(1))) return rc;
+    } else if ((rc = h->ensure_scratch(0, 2))) {  // fields 0, 3, 4, 5 of the 2-item scratch
+        return rc;
+    }
+    cudaEvent_t ev[5];
+    for (auto& e : ev) SP_CUDA(cudaEventCreate(&e));
+    cudaError_t e = cudaSuccess;
+    if (fused) {
+        e = launch_widen(h->g4, h->wbuf(0, 1), g, field, 1, nullptr, 0, s);
+        PairLaunch L;
+        L.nu = nu; L.dt = dt; L.coef = h->coef;
+        for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+            void* Q = h->wbuf(r % 2, 1);
+            void* A = h->wbuf((r + 1) % 2, 1);
+            L.pair = 0; L.q = Q; L.y2 = h->wbuf(2, 1); L.acc = A; L.out = A;
+            cudaEventRecord(ev[0], s);
+            e = launch_pair(h->g4, h->g4, L, t.pair[0], s, err);
+            cudaEventRecord(ev[1], s);
+            L.pair = 1;
+            if (e == cudaSuccess) e = launch_pair(h->g4, h->g4, L, t.pair[1], s, err);
+            cudaEventRecord(ev[2], s);
+            cudaEventSynchronize(ev[2]);
+            float m0 = 0, m1 = 0;
+            cudaEventElapsedTime(&m0, ev[0], ev[1]);
+            cudaEventElapsedTime(&m1, ev[1], ev[2]);
+            acc[0] += m0; acc[1] += m1;
+        }
+        *count = 2;
+    } else {
+        void* q = h->sbuf(0, 3, 1);
+        void* ya = h->sbuf(0, 4, 1);
+        void* yb = h->sbuf(0, 5, 1);
+        void* ac = h->sbuf(0, 0, 1);
+        e = cudaMemcpyAsync(q, field, g.total * g.es, cudaMemcpyDeviceToDevice, s);
+        StageLaunch L;
+        L.prec = 0; L.items = 1; L.nu = nu; L.coef = h->coef;
+        const double dthalf = dt * .5;
+        const int op[4] = {OP_RK_S1, OP_RK_S2, OP_RK_S3, OP_RK_S4};
+        const void* yin[4] = {q, ya, yb, ya};
+        void* yout[4] = {ya, yb, ya, q};
+        const double cy[4] = {dthalf, dthalf, dt, 0.}, ca[4] = {dt / 6., dt / 3., dt / 3., dt / 6.};
+        for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+            cudaEventRecord(ev[0], s);
+            for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+                L.op = op[k]; L.yin = yin[k]; L.yout = yout[k]; L.acc = ac; L.q = (k == 1 || k == 2) ? q : nullptr;
+                L.c_y = cy[k]; L.c_acc = ca[k];
+                e = launch_stage(g, L, t, s, err);
+                cudaEventRecord(ev[k + 1], s);
+            }
+            cudaEventSynchronize(ev[4]);
+            for (int k = 0; k < 4; ++k) {
+                float m = 0;
+                cudaEventElapsedTime(&m, ev[k], ev[k + 1]);
+                acc[k] += m;
+            }
+        }
+        *count = 4;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "kernel timing: %s", cudaGetErrorString(e));
+    for (int k = 0; k < *count; ++k) ms[k] = acc[k] / reps;
+    return sp_convection_synchronize(h);
+}
+
+// ---------------------------------------------------------------------------
 // Autotuner: for every stage kernel (RK4 S1..S4, Euler) times each candidate
 // launch shape (kernel kind x tile rows x z-chunk) on scratch fields and keeps
 // the fastest shape per stage.
