@@ -846,7 +846,8 @@ struct sp_parareal {
     Geo g64, gc;
     DevBuf U;              // P+1 FP64 fields: slice inputs U_0..U_{P-1}, last slice result U_P
     DevBuf F;              // P FP64 fields: fine results
-    DevBuf fs;             // 3P FP64 fields: fine scratch ya, yb, acc
+    DevBuf fs;             // 3P FP64 fields: fine scratch ya, yb, acc (single-stage F sweep)
+    DevBuf fw;             // 3P fields of geometry g4: step start / accumulator x2, y2 (fused F sweep)
     DevBuf Gold;           // P coarse fields (reference form of the correction)
     DevBuf D;              // P+1 coarse fields: slice increments (increment form)
     DevBuf Gt;             // 2 coarse fields (coarse result / ping-pong) + 3 coarse scratch
@@ -927,16 +928,47 @@ int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long*
     const Geo& g = pr->g64;
     const Tune tf = h->tune(0, P);
     int* err = h->err.as<int>();
+    const bool const_nu = h->P.nufreq == 0.;
+    // F sweep as fused stage pairs when the tune says so and one nu serves all
+    // slices; scratch for the chosen path, allocated before the capture
+    const bool fused = const_nu && tf.fused && pair_supported(h->g4);
+    const Geo& g4 = h->g4;
+    if ((parts & 1) && (fused ? pr->fw.alloc((size_t)3 * P * g4.total * g4.es)
+                              : pr->fs.alloc((size_t)3 * P * g.total * g.es)) != cudaSuccess)
+        return fail(SP_ERR_NOMEM, "fine-sweep scratch for %d slices", P);
     const size_t fstride = (size_t)P * g.total;
     double* ya = pr->fs.as<double>();
     double* yb = ya + fstride;
     double* acc = yb + fstride;
-    const bool const_nu = h->P.nufreq == 0.;
     SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     const long long before = launches();
     int rc = SP_OK;
     cudaError_t e = events ? cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal) : cudaSuccess;
-    for (int i = 0; i < pr->tsF && e == cudaSuccess && (parts & 1); ++i) {
+    if (fused && (parts & 1)) {
+        // widen the slice inputs once, alternate step start / accumulator
+        // between W0 and W1, write the last step into the fine results
+        const size_t w4 = (size_t)P * g4.total;
+        double* W0 = pr->fw.as<double>();
+        double* W1 = W0 + w4;
+        double* WY = W1 + w4;
+        if (e == cudaSuccess) e = launch_widen(g4, W0, g, pr->u(0), P, pr->itemlo(), 0, s);
+        PairLaunch L;
+        L.items = P;
+        L.item_lo = pr->itemlo();
+        L.nu = h->P.nu0;
+        L.dt = pr->dtF;
+        L.coef = h->coef;
+        for (int i = 0; i < pr->tsF && e == cudaSuccess; ++i) {
+            double* Q = (i % 2) ? W1 : W0;
+            double* A = (i % 2) ? W0 : W1;
+            const bool last = i + 1 == pr->tsF;
+            L.pair = 0; L.q = Q; L.y2 = WY; L.acc = A;
+            e = launch_pair(g4, g4, L, tf.pair[0], s, err);
+            L.pair = 1; L.out = last ? (void*)pr->f(0) : (void*)A;
+            if (e == cudaSuccess) e = launch_pair(g4, last ? g : g4, L, tf.pair[1], s, err);
+        }
+    }
+    for (int i = 0; i < pr->tsF && e == cudaSuccess && (parts & 1) && !fused; ++i) {
         NuSrc nu;
         if (const_nu) nu.nu = h->P.nu0;
         else nu.items = pr->nutab.as<double>() + (size_t)i * P;
@@ -1077,7 +1109,6 @@ int sp_parareal_create(sp_convection* prop, const sp_parareal_cfg* cfg, sp_parar
     const size_t cb = (size_t)pr->gc.total * pr->gc.es;
     const bool delta = c.coarse_delta != 0;
     if (pr->U.alloc((P + 1) * f64b) != cudaSuccess || pr->F.alloc(P * f64b) != cudaSuccess ||
-        pr->fs.alloc(3 * P * f64b) != cudaSuccess ||
         (delta ? pr->D.alloc((P + 1) * cb) : pr->Gold.alloc(P * cb)) != cudaSuccess || pr->Z.alloc(cb) != cudaSuccess ||
         pr->Gt.alloc(5 * cb) != cudaSuccess || pr->ctl.alloc(256 + (2 * P + 8) * sizeof(double)) != cudaSuccess)
         return fail(SP_ERR_NOMEM, "Parareal state for %d slices", P);

@@ -124,3 +124,24 @@ def test_fused_batch_autotune_picks_a_valid_shape(sp):
     else:  # the tuner may pick direct-load stage kernels (difference form of the update)
         assert rel_l2(got, ref) < 1e-13
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("skip", [True, False])
+def test_parareal_fine_sweep_fused_equals_single_stage(sp, skip):
+    """The batched F sweep of Parareal (all slices per launch, converged slices
+    skipped) gives the same fields with fused pairs as with single-stage kernels."""
+    n, P = 20, 4
+    outs = []
+    for tune in (SINGLE, (8, 0, 2)):
+        conv = sp.Convection(n, n, n, 1.0 / n, 0.05, 0.0, 1.0, 0.5, -0.25)
+        conv.set_tune(sp.SP_F64, P, *tune)
+        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.02, timeStepsFine=160,
+                                       timeStepsCoarse=12, kmax=3)
+        fin, fsol = conv.field(), conv.field()
+        conv.upload(fin, gaussian_noise(n, seed=11))
+        par = sp.Parareal(conv, fin, fsol, 0.0, conf, coarse="rk4", coarse_precision="f64", skip_converged=skip)
+        par.DoParallel()
+        outs.append(conv.download(fsol))
+        cfg = conv.tuned_configs(sp.SP_F64, P)
+        assert cfg["P12"]["kind"] == (2 if tune[2] == 2 else 0)
+    assert np.array_equal(outs[0], outs[1])
