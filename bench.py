@@ -234,7 +234,9 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
     for i, (n, nu, c, P) in enumerate(specs):
         conv = sp.Convection(n, n, n, 1.0 / n, nu, 0.0, *c, device=device)
         if n not in tunes:
-            tunes[n] = (conv.autotune(sp.SP_F64, 16)["S2"], conv.autotune(sp.SP_F32, 1)["S2"])
+            a64 = conv.autotune(sp.SP_F64, 16)
+            # fused stage pairs when the tuner preferred them, else the stage kernels' shape
+            tunes[n] = (a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"], conv.autotune(sp.SP_F32, 1)["S2"])
         t64, t32 = tunes[n]
         conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
         conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
