@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 
 #include "sp_device.cuh"
 #include "sp_internal.h"
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const bool leader = tid == 0;
 
+    pdl_trigger();  // the next kernel's CTAs may start as this grid's CTAs retire
     if (leader) {
         prefetch_tensormap(&tm_s);
 #pragma unroll
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
         fence_mbar_init();
     }
     __syncthreads();
+    pdl_wait();     // fields written by the previous kernel are read from here on
 
     // own cells and ring chunk
     const bool has_h = tid < NH;
@@ -413,11 +416,31 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
 
 
 
+// Launches a kernel with programmatic stream serialization (the kernels here
+// call pdl_trigger/pdl_wait), so that in a stream or a captured graph the
+// next kernel's CTAs start while this one's last CTAs finish.
+template <typename... KP, typename... A>
+cudaError_t launch_pdl(void (*k)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 // ---------------------------------------------------------------------------
 // Widening: interior of a caller-layout field -> internal field with every
 // periodic image within 4 cells of a face.
 __global__ void k_widen(double* dst, Geo gd, const double* src, Geo gs, int items, const int* item_lo,
                         int item_base) {
+    pdl_trigger();
+    pdl_wait();
     const long long n = (long long)gd.ni * gd.nj * gd.nk;
     const int b = blockIdx.y;
     if (item_lo && b + item_base < *item_lo) return;
@@ -494,8 +517,7 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     const long long nct = (total + a.span - 1) / a.span;
     if (nct > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     const dim3 grid((unsigned)nct);
-    k_rk4_pair<PAIR, TY, NSQ, NP><<<grid, 32 * TY, S::smem, s>>>(ts, tq, ta, a);
-    return cudaGetLastError();
+    return launch_pdl(k_rk4_pair<PAIR, TY, NSQ, NP>, grid, dim3(32 * TY), S::smem, s, ts, tq, ta, a);
 }
 
 template <int PAIR, int TY, int NSQ, int NP>
@@ -540,9 +562,8 @@ cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* sr
     add_launches(1);
     if (g4.es != 8 || gs.es != 8 || items < 1 || items > 65535) return cudaErrorInvalidValue;
     dim3 grid(grid_cells((long long)g4.ni * g4.nj * g4.nk), items);
-    k_widen<<<grid, 256, 0, s>>>(static_cast<double*>(dst), g4, static_cast<const double*>(src), gs, items, item_lo,
-                                 item_base);
-    return cudaGetLastError();
+    return launch_pdl(k_widen, grid, dim3(256), 0, s, static_cast<double*>(dst), g4,
+                      static_cast<const double*>(src), gs, items, item_lo, item_base);
 }
 
 }  // namespace sp
