@@ -407,14 +407,26 @@ def main():
     alg_launch = KERNEL_BYTES[dom] * n ** 3
     achieved = alg_launch / (ktimes[dom] * 1e-3) / 1e9
     step_bytes = sum(KERNEL_BYTES[k] for k in ktimes)
-    traffic = None
+    traffic_tab = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch", {}).get(dom)
+                traffic_tab = json.load(f).get("dram_bytes_per_launch", {})
         except Exception:
-            traffic = None
+            traffic_tab = {}
+    traffic = traffic_tab.get(dom)
+    # the four single-stage kernels on the same field, for comparison: they move
+    # 128 B per cell-update against the pairs' 56 B and are bound by HBM
+    st = conv.kernel_times(fin, DT, reps=20, path="stages")
+    sdom = max(st, key=st.get)
+    s_ach = KERNEL_BYTES[sdom] * n ** 3 / (st[sdom] * 1e-3) / 1e9
+    s_step = sum(KERNEL_BYTES[k] for k in st) * n ** 3 / (sum(st.values()) * 1e-3) / 1e9
+    roofline_single = {"bound": "hbm", "kernel": KERNEL_NAMES[sdom], "achieved": s_ach, "peak": peak, "unit": "GB/s",
+                       "frac": s_ach / peak, "traffic": traffic_tab.get(sdom), "kernel_times_ms": st,
+                       "step_achieved_gbs": s_step, "step_frac": s_step / peak,
+                       "step_gcups": n ** 3 / (sum(st.values()) * 1e-3) / 1e9,
+                       "pairs_step_gcups": n ** 3 / (sum(ktimes.values()) * 1e-3) / 1e9}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -426,6 +438,7 @@ def main():
                          "algorithmic_bytes_per_launch": alg_launch, "kernel_ms": ktimes[dom],
                          "kernel_times_ms": ktimes, "algorithmic_bytes_per_cell_update": step_bytes,
                          "step_achieved_gbs": step_bytes * n ** 3 * STEPS_PER_RUN * args.steps / t_local / 1e9},
+            "roofline_single_stage": roofline_single,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8)},
             "gpu_launches": int(launches), "clocks": clk.summary()}

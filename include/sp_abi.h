@@ -256,10 +256,11 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
 int sp_autotune(sp_convection* h, int precision, int batch);
 /* Average duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
  * events around every launch on the handle's stream over `reps` steps run on a
- * copy of `field` (which is left unchanged).  *count = 2 (ms[0..1]: fused
- * pairs 1+2, 3+4) or 4 (ms[0..3]: stages S1..S4), per the handle's tune.
+ * copy of `field` (which is left unchanged).  path 0: the kernels the handle's
+ * tune runs, 1: the four stage kernels (tuned shapes), 2: the fused pairs.
+ * *count = 2 (ms[0..1]: pairs 1+2, 3+4) or 4 (ms[0..3]: stages S1..S4).
  * Measurement support, no counterpart in the reference. */
-int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, float* ms, int* count);
+int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, int path, float* ms, int* count);
 /* Forces one launch shape for a precision and batch.  kind 0 or 1: every
  * single-stage kernel, ty in {4,8,16}, zchunk >= 1, RK4 steps unfused.  kind 2
  * (FP64): RK4 steps as fused pairs with ty in {8,16} and zchunk planes per CTA

@@ -199,13 +199,15 @@ class Convection:
         L.check(L.lib().sp_tuned_config(self._h, precision, batch, op, C.byref(ty), C.byref(zc), C.byref(tma)))
         return {"ty": ty.value, "zchunk": zc.value, "kind": tma.value}
 
-    def kernel_times(self, field: ConvectionField, dt: float, reps: int = 10):
+    def kernel_times(self, field: ConvectionField, dt: float, reps: int = 10, path: str = "tuned"):
         """Average ms of each kernel of an FP64 RK4 step (CUDA events on the
-        library's stream), run on a copy of `field`: {"P12", "P34"} when steps
-        run as fused pairs, else {"S1".."S4"}."""
+        library's stream), run on a copy of `field`: {"P12", "P34"} for the fused
+        pairs, {"S1".."S4"} for the stage kernels.  path: "tuned" (what DoRK4
+        runs), "stages" or "pairs"."""
         ms = (C.c_float * 4)()
         cnt = C.c_int()
-        self.call(L.lib().sp_kernel_times, self._h, C.c_void_p(field.ptr), dt, reps, ms, C.byref(cnt))
+        code = {"tuned": 0, "stages": 1, "pairs": 2}[path]
+        self.call(L.lib().sp_kernel_times, self._h, C.c_void_p(field.ptr), dt, reps, code, ms, C.byref(cnt))
         names = ("P12", "P34") if cnt.value == 2 else ("S1", "S2", "S3", "S4")
         return {k: float(ms[i]) for i, k in enumerate(names)}
 

@@ -646,10 +646,11 @@ int sp_field_errors(sp_convection* h, const double* a, const double* b, double* 
 // ---------------------------------------------------------------------------
 // Per-kernel durations of FP64 RK4 steps (CUDA events around every launch on
 // the handle's stream), on a copy of `field`; the field is not modified.
-extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, float* ms, int* count) {
+extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, int path, float* ms,
+                               int* count) {
     int rc = check_handle(h);
     if (rc) return rc;
-    if (!field || !ms || !count || reps < 1) return fail(SP_ERR_INVALID, "bad arguments");
+    if (!field || !ms || !count || reps < 1 || path < 0 || path > 2) return fail(SP_ERR_INVALID, "bad arguments");
     cudaStream_t s = h->stream();
     if (capturing(s)) return fail(SP_ERR_STATE, "cannot time kernels while the stream is capturing");
     const Tune t = h->tune(0, 1);
@@ -657,7 +658,8 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
     const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
     int* err = h->err.as<int>();
     float acc[4] = {0, 0, 0, 0};
-    const bool fused = t.fused && pair_supported(h->g4);
+    if (path == 2 && !pair_supported(h->g4)) return fail(SP_ERR_INVALID, "fused pairs need >= 4 cells per axis");
+    const bool fused = path == 2 || (path == 0 && t.fused && pair_supported(h->g4));
     if (fused) {
         if ((rc = h->ensure_wide(1))) return rc;
     } else if ((rc = h->ensure_scratch(0, 2))) {  // fields 0, 3, 4, 5 of the 2-item scratch

@@ -145,3 +145,18 @@ def test_parareal_fine_sweep_fused_equals_single_stage(sp, skip):
         cfg = conv.tuned_configs(sp.SP_F64, P)
         assert cfg["P12"]["kind"] == (2 if tune[2] == 2 else 0)
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_kernel_times_paths_leave_field_unchanged(sp):
+    n = (32, 32, 32)
+    c = make(sp, n)
+    f = c.field()
+    c.upload(f, gaussian_noise(*n, seed=12))
+    before = f.data.clone()
+    kp = c.kernel_times(f, 1e-4, reps=2, path="pairs")
+    ks = c.kernel_times(f, 1e-4, reps=2, path="stages")
+    kt = c.kernel_times(f, 1e-4, reps=2)
+    assert set(kp) == {"P12", "P34"} and set(kt) == {"P12", "P34"}
+    assert set(ks) == {"S1", "S2", "S3", "S4"}
+    assert all(v > 0 for v in list(kp.values()) + list(ks.values()))
+    assert torch.equal(f.data, before)
