@@ -268,7 +268,11 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
         const bool full = x + 2 <= a.ni;
         // whether the cells have periodic images in x or y (image depth hd)
         const int hd = PAIR == 0 ? 4 : a.o_halo;
-        const bool xy_img = x < hd || x + 2 > a.ni - hd || y < hd || y >= a.nj - hd || !full;
+        // lanes next to an x face add their x-images to the 16-byte store; rows
+        // and planes next to a y or z face (and an odd ni's last pair) take the
+        // general image path
+        const bool x_img = x < hd || x + 2 > a.ni - hd;
+        const bool y_img = y < hd || y >= a.nj - hd || !full;
         // the own cells' output columns at plane z0-4 (one plane further per iteration)
         double* ocol;
         [[maybe_unused]] double* acol = nullptr;
@@ -363,21 +367,26 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
                 }
                 if (live) {
                     const int z = z0 - 4 + v;
-                    const bool inner = !xy_img && z >= hd && z < a.nk - hd;
+                    if (!y_img && z >= hd && z < a.nk - hd) {
+                        st16<double>(ocol, o);
+                        if (x_img) {
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const int xe = x + e;
+                                if (xe < hd) ocol[e + a.ni] = o.v[e];
+                                if (xe >= a.ni - hd) ocol[e - a.ni] = o.v[e];
+                            }
+                        }
+                    } else if constexpr (PAIR == 0) {
+                        store_images_pair(a.yout + (long long)b * a.item_stride + a.origin, a.px, a.plane, a.ni,
+                                          a.nj, a.nk, 4, x, y, z, o);
+                    } else {
+                        store_images_pair(a.qout + (long long)b * a.o_item_stride + a.o_origin, a.o_px, a.o_plane,
+                                          a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
+                    }
                     if constexpr (PAIR == 0) {
-                        if (inner)
-                            st16<double>(ocol, o);
-                        else
-                            store_images_pair(a.yout + (long long)b * a.item_stride + a.origin, a.px, a.plane, a.ni,
-                                              a.nj, a.nk, 4, x, y, z, o);
                         if (full) st16<double>(acol, oa);
                         else acol[0] = oa.v[0];
-                    } else {
-                        if (inner)
-                            st16<double>(ocol, o);
-                        else
-                            store_images_pair(a.qout + (long long)b * a.o_item_stride + a.o_origin, a.o_px,
-                                              a.o_plane, a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
                     }
                 }
             }
