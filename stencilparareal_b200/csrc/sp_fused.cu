@@ -48,7 +48,8 @@ struct PairArgs {
     long long item_stride, origin, px, plane;  // internal geometry (4-cell halo)
     int ni, nj, nk, pz;
     int tiles_x, tiles_y, items;
-    int span;          // planes of the flattened (tile, z) space per CTA (total < 2^31)
+    int cy;            // CTAs per group: y-adjacent tiles marching the same plane range
+    int span;          // planes of the flattened (tile group, z) space per group (total < 2^31)
     const int* item_lo;
     int item_base;
     W13<double> w;
@@ -195,21 +196,29 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     // This CTA's planes: [g_lo, g_hi) of all (tile, z) planes, tiles ordered x
     // fastest, then y, then item.  A segment is the part inside one tile; each
     // segment pays 4 extra plane iterations to fill the pipeline.
-    const int tiles_xy = a.tiles_x * a.tiles_y;
-    const int total = tiles_xy * a.items * a.nk;
-    const int g_lo = blockIdx.x * a.span;
+    // Groups of cy consecutive CTAs take y-adjacent tiles (same x tile, same
+    // item) over the same plane range; the grid is one wave, so a group's
+    // CTAs march their planes together and the halo rows they share are read
+    // from HBM once.
+    const int groups_y = (a.tiles_y + a.cy - 1) / a.cy;
+    const int groups_xy = a.tiles_x * groups_y;
+    const int total = groups_xy * a.items * a.nk;
+    const int member = blockIdx.x % a.cy;
+    const int g_lo = (blockIdx.x / a.cy) * a.span;
     const int g_hi = min(g_lo + a.span, total);
     unsigned U = 0, VP = 0;  // stencil / pointwise planes this CTA has loaded: ring positions
     for (int g = g_lo; g < g_hi;) {
-        const int tile = g / a.nk;
-        const int z0 = g - tile * a.nk;
+        const int grp = g / a.nk;
+        const int z0 = g - grp * a.nk;
         const int z1 = min(a.nk, z0 + (g_hi - g));
         g += z1 - z0;
-        const int b = tile / tiles_xy;
-        const int txy = tile - b * tiles_xy;
+        const int b = grp / groups_xy;
+        const int gxy = grp - b * groups_xy;
+        const int ty = (gxy / a.tiles_x) * a.cy + member;
+        if (ty >= a.tiles_y) continue;                             // a partial group's spare CTA
         if (a.item_lo && b + a.item_base < *a.item_lo) continue;  // the same for all threads
-        const int x0 = (txy % a.tiles_x) * TX;
-        const int y0 = (txy / a.tiles_x) * TY;
+        const int x0 = (gxy % a.tiles_x) * TX;
+        const int y0 = ty * TY;
         const int nv = z1 - z0 + 4;      // first-stage planes z0-2 .. z1+1
         const int nu = z1 - z0 + 8;      // stencil planes z0-4 .. z1+3
         const int zs = b * a.pz + z0;    // tensor-map plane of stencil plane 0 (interior z0-4)
@@ -496,7 +505,8 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     a.tiles_x = (g4.ni + S::TX - 1) / S::TX;
     a.tiles_y = (g4.nj + TY - 1) / TY;
     a.items = L.items;
-    const long long total = (long long)a.tiles_x * a.tiles_y * L.items * g4.nk;
+    a.cy = a.tiles_y % 4 == 0 ? 4 : (a.tiles_y % 2 == 0 ? 2 : 1);
+    const long long total = (long long)a.tiles_x * (a.tiles_y / a.cy + (a.tiles_y % a.cy != 0)) * L.items * g4.nk;
     if (total >= 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     if (sh.zchunk > 0) {
         a.span = sh.zchunk;
@@ -505,7 +515,7 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP>, 32 * TY, S::smem);
-        const long long ctas = (long long)std::max(1, sms) * std::max(1, occ);
+        const long long ctas = std::max(1LL, (long long)std::max(1, sms) * std::max(1, occ) / a.cy);  // groups
         a.span = (int)std::max(1LL, (total + ctas - 1) / ctas);
     }
     a.item_lo = L.item_lo;
@@ -523,7 +533,7 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
         a.o_halo = go.halo;
     }
     a.err = err;
-    const long long nct = (total + a.span - 1) / a.span;
+    const long long nct = (total + a.span - 1) / a.span * a.cy;
     if (nct > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     const dim3 grid((unsigned)nct);
     return launch_pdl(k_rk4_pair<PAIR, TY, NSQ, NP>, grid, dim3(32 * TY), S::smem, s, ts, tq, ta, a);
