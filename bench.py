@@ -173,6 +173,43 @@ def cpu_baseline_sample():
             "sample": f"{steps} RK4 steps of {n}^3 (oracle restating the reference OpenMP path), {dt:.1f} s"}
 
 
+def cpu_config_times(torch, sp, device, gpu_c3_serial_s=None):
+    """CPU (oracle, all host cores) beside GPU times for config 1 in full (32^3, 1000 RK4
+    steps) and for config 3's serial fine propagator (128^3, 20000 steps; CPU on 200
+    steps, extrapolated)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import gaussian_noise
+    from oracle import oracle as O
+    O.build()
+    O.set_threads(os.cpu_count() or 1)
+    out = {"cores": O.get_threads()}
+    n, steps, dt = 32, 1000, 1e-4
+    q0 = gaussian_noise(n, seed=0)
+    p = O.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
+    t0 = time.perf_counter()
+    O.rk4(p, q0, 0.0, dt, steps)
+    cpu = time.perf_counter() - t0
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+    fi, fo = conv.field(), conv.field()
+    conv.upload(fi, q0)
+    conv.DoRK4(fi, fo, 0.0, dt, steps)
+    conv.synchronize()
+    t0 = time.perf_counter()
+    conv.DoRK4(fi, fo, 0.0, dt, steps)
+    conv.synchronize()
+    gpu = time.perf_counter() - t0
+    out["config1"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01", "cpu_s": cpu, "gpu_s": gpu}
+    n, sample, total = 128, 200, 20000
+    p = O.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
+    q0 = gaussian_noise(n, seed=0)
+    t0 = time.perf_counter()
+    O.rk4(p, q0, 0.0, 1e-5, sample)
+    cpu = time.perf_counter() - t0
+    out["config3_serial_fine"] = {"what": "128^3, 20000 RK4 FP64 steps, dt=1e-5", "cpu_s_extrapolated": cpu * total / sample,
+                                  "cpu_sample": f"{sample} of {total} steps in {cpu:.2f} s", "gpu_s": gpu_c3_serial_s}
+    return out
+
+
 def parareal_summary(torch, sp, device):
     """Config 3: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -451,6 +488,11 @@ def main():
                     line[key] = {"error": repr(ex)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample()
+            try:
+                line["cpu_configs"] = cpu_config_times(torch, sp, device,
+                                                       line.get("parareal", {}).get("serial_fine_s"))
+            except Exception as ex:  # reported, not hidden
+                line["cpu_configs"] = {"error": repr(ex)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
