@@ -20,13 +20,19 @@
 //
 // CTA: 32*TY threads; thread (warp w, lane l) owns cells (x0+2l, x0+2l+1) of
 // tile row y0+w (tile 64 x TY), and threads below NH also one 2-cell chunk of
-// the 2-cell ring around the tile.  The CTA marches a chunk of z-planes:
+// the ring around the tile (two rows above and below over the tile's columns,
+// two columns left and right over its rows).  The grid is persistent (one
+// wave): groups of up to 4 CTAs take y-adjacent tiles over one range of
+// planes, so that they march together and share their halo rows through L2;
+// a range is cut into segments at tile boundaries.  In a segment [z0, z1)
 // iteration v evaluates the first stage on plane z0-2+v and the second on
 // plane z0-4+v.  Shared memory: NSQ slots of the stencil input (TMA boxes of
 // (64+8) x (TY+8) cells), 3 slots of the widened first-stage field, NP slots
 // of pointwise operands (pair 3+4: q on the widened tile and acc on the tile),
 // and the mbarriers of the TMA slots.  z-neighbours of the thread's own cells
-// are carried in registers; the ring cells read theirs from the slots.
+// are carried in registers; the ring cells read theirs from the slots.  The
+// kernels are launched with programmatic dependent launch and read global
+// memory only after griddepcontrol.wait.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
