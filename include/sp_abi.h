@@ -254,6 +254,12 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
  * stage kernel gets the fastest of its candidate launch shapes, and FP64 RK4
  * steps run as fused pairs when those are faster than the four stages. */
 int sp_autotune(sp_convection* h, int precision, int batch);
+/* Test of the error path of the bounded in-kernel waits: runs one kernel whose
+ * wait can never complete and gives up after limit_ms (<= 2000); returns
+ * SP_ERR_TIMEOUT, as any kernel of the library would after a wait expires,
+ * and leaves the handle usable.  No counterpart in the reference (which has
+ * no bounded waits). */
+int sp_selftest_wait_timeout(sp_convection* h, double limit_ms);
 /* Average duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
  * events around every launch on the handle's stream over `reps` steps run on a
  * copy of `field` (which is left unchanged).  path 0: the kernels the handle's

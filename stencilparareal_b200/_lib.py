@@ -99,6 +99,7 @@ _SIGS = {
     "sp_autotune": (_i, [_vp, _i, _i]),
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
     "sp_kernel_times": (_i, [_vp, _vp, C.c_double, _i, _i, C.POINTER(C.c_float), C.POINTER(_i)]),
+    "sp_selftest_wait_timeout": (_i, [_vp, C.c_double]),
     "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),
     "sp_parareal_window_begin": (_i, [_vp, _vp]),
     "sp_parareal_window_fine": (_i, [_vp, _i]),

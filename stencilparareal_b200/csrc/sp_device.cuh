@@ -56,13 +56,14 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-// Waits for phase `parity` of the barrier; false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Waits for phase `parity` of the barrier; false after limit_ns.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
+        if ((it & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
     }
 }
 

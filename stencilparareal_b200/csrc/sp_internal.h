@@ -114,6 +114,9 @@ cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const
 cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* src, int items, const int* item_lo,
                          int item_base, cudaStream_t s);
 cudaError_t prepare_pairs();
+// One CTA waiting on an mbarrier that never completes, bounded by limit_ns;
+// sets *err to the timeout code (test of the bounded-wait error path).
+cudaError_t launch_wait_selftest(int* err, unsigned long long limit_ns, cudaStream_t s);
 
 // Pointwise helpers.
 cudaError_t launch_periodicity(const Geo& g, void* field, int items, cudaStream_t s);

@@ -707,6 +707,28 @@ cudaError_t prepare_kernels() {
     return e;
 }
 
+namespace {
+// Self-test of the bounded waits: one CTA waits on an mbarrier that nothing
+// arrives on, gives up after limit_ns like every pipeline wait, records the
+// timeout in the device error word and returns.
+__global__ void k_wait_selftest(int* err, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicExch(err, DEV_WAIT_TIMEOUT);
+}
+}  // namespace
+
+cudaError_t launch_wait_selftest(int* err, unsigned long long limit_ns, cudaStream_t s) {
+    add_launches(1);
+    k_wait_selftest<<<1, 64, 0, s>>>(err, limit_ns);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stage(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err) {
     add_launches(1);
     if (L.op < 0 || L.op >= kNumOps) return cudaErrorInvalidValue;

@@ -644,6 +644,18 @@ int sp_field_errors(sp_convection* h, const double* a, const double* b, double* 
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Error-path self-test: a kernel whose wait can never complete gives up after
+// limit_ms; the call returns the status the handle then reports (SP_ERR_TIMEOUT)
+// and leaves the handle usable.
+extern "C" int sp_selftest_wait_timeout(sp_convection* h, double limit_ms) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!(limit_ms > 0.) || limit_ms > 2000.) return fail(SP_ERR_INVALID, "limit_ms must be in (0, 2000]");
+    SP_CUDA(launch_wait_selftest(h->err.as<int>(), (unsigned long long)(limit_ms * 1e6), h->stream()));
+    return sp_convection_synchronize(h);
+}
+
+// ---------------------------------------------------------------------------
 // Per-kernel durations of FP64 RK4 steps (CUDA events around every launch on
 // the handle's stream), on a copy of `field`; the field is not modified.
 extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, int path, float* ms,

@@ -82,3 +82,26 @@ def test_mat_output_of_both_drivers(tmp_path, monkeypatch):
     m = scipy.io.loadmat("result.mat")
     assert m["q"].shape == (12, 12, 12)
     np.testing.assert_allclose(m["q"], m["qreference"], rtol=0, atol=1e-12)
+
+
+def test_bounded_wait_timeout_reports_and_recovers(sp, orc):
+    """A kernel wait that can never complete gives up after its limit, the call
+    returns SP_ERR_TIMEOUT, and the handle keeps working."""
+    import time
+    L = sp._lib
+    lib = L.lib()
+    n = 16
+    c = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0)
+    t0 = time.perf_counter()
+    rc = lib.sp_selftest_wait_timeout(c.handle, 50.0)
+    assert rc == L.SP_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    assert lib.sp_selftest_wait_timeout(c.handle, 0.0) == L.SP_ERR_INVALID
+    from ics import gaussian_noise, rel_l2
+    q0 = gaussian_noise(n, seed=4)
+    f, g = c.field(), c.field()
+    c.upload(f, q0)
+    c.DoRK4(f, g, 0.0, 1e-4, 5)
+    c.synchronize()
+    ref = orc.rk4(orc.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0), q0, 0.0, 1e-4, 5)
+    assert rel_l2(c.download(g), ref) < 1e-12
