@@ -47,8 +47,9 @@ NU = 1e-3
 C = (1.0, 0.5, 0.25)
 # Algorithmic HBM bytes per cell of each kernel of an RK4 step (FP64 field
 # accesses x 8 B): fused pairs 1+2 (q -> y2, acc) and 3+4 (y2, q, acc -> q'),
-# or the four single-stage kernels.
-KERNEL_BYTES = {"P12": 24, "P34": 32, "S1": 24, "S2": 40, "S3": 40, "S4": 24}
+# 56 B per cell-update, or the four single-stage kernels S1 (q -> y1),
+# S2 (y1, q -> y2, acc), S3 (y2, q -> y3), S4 (y3, acc, q -> q'), 104 B.
+KERNEL_BYTES = {"P12": 24, "P34": 32, "S1": 16, "S2": 32, "S3": 24, "S4": 32}
 KERNEL_NAMES = {"P12": "k_rk4_pair<0,...> (RK4 stages 1+2)", "P34": "k_rk4_pair<1,...> (RK4 stages 3+4)",
                 "S1": "k_stage_tma<double,0,...>", "S2": "k_stage_tma<double,1,...>",
                 "S3": "k_stage_tma<double,2,...>", "S4": "k_stage_tma<double,3,...>"}
@@ -454,7 +455,7 @@ def main():
             traffic_tab = {}
     traffic = traffic_tab.get(dom)
     # the four single-stage kernels on the same field, for comparison: they move
-    # 128 B per cell-update against the pairs' 56 B and are bound by HBM
+    # 104 B per cell-update against the pairs' 56 B and are bound by HBM
     st = conv.kernel_times(fin, DT, reps=20, path="stages")
     sdom = max(st, key=st.get)
     s_ach = KERNEL_BYTES[sdom] * n ** 3 / (st[sdom] * 1e-3) / 1e9

@@ -7,8 +7,10 @@
 // stencil radius (2 cells in x and y, 2 planes ahead in z) and kept in shared
 // memory, where the second stage reads it.  Per step the pairs move 7 values
 // per cell (56 B):
-//   pair 1+2: reads q;           writes y2 = q + dt/2 R(y1), acc = q + dt/6 k1 + dt/3 k2
-//   pair 3+4: reads y2, q, acc;  writes q' = acc + dt/3 k3 + dt/6 k4
+//   pair 1+2: reads q;           writes y2 = q + dt/2 R(y1), acc = q + (y1 - q)/3 + dt/3 k2
+//   pair 3+4: reads y2, q, acc;  writes q' = acc + (y3 - q)/3 + dt/6 k4
+// ((y1 - q)/3 = dt/6 k1 and (y3 - q)/3 = dt/3 k3: the forms the single-stage
+// kernels use, where they save the accumulator traffic of stages 1 and 3)
 // Every value is computed with the same operations, in the same order, as the
 // single-stage kernels, so both paths give bit-identical fields.
 //
@@ -59,8 +61,8 @@ struct PairArgs {
     const int* item_lo;
     int item_base;
     W13<double> w;
-    double c1y, c1a;   // first stage:  y = c1y k + base, a = c1a k + abase
-    double c2y, c2a;   // second stage
+    double c1y;        // first stage:  y = c1y k + base
+    double c2y, c2a;   // second stage: y = c2y k + q (pair 1+2), acc / result = c2a k + base
     double* yout;      // pair 1+2: y2 (internal geometry, images 4 deep)
     double* aout;      // pair 1+2: acc (internal geometry, interior only)
     double* qout;      // pair 3+4: step result
@@ -264,7 +266,8 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
         //   ew[p % 5]: first-stage value at first-stage plane p (p = v-4 .. v)
         //   aw[p % 5]: first-stage accumulator partial (p = v-2 .. v)
         //   sa[u % 5]: shared address of the slot of stencil plane u
-        V2 qw[5], ew[5], aw[5];
+        V2 qw[5], ew[5];
+        [[maybe_unused]] V2 aw[5];  // pair 3+4 only
         uint32_t sa[5];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {  // prologue: stencil planes 0..3
@@ -328,26 +331,25 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
             {
                 double k[2];
                 rhs_s<WB>(a.w, S2 + m_s8, qw[(K + 2) % 5], qw[K], qw[(K + 1) % 5], qw[(K + 3) % 5], qw[(K + 4) % 5], k);
-                V2 en, an;
+                V2 en;
                 if constexpr (PAIR == 0) {
                     const V2& c = qw[(K + 2) % 5];
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        en.v[e] = fmaT(a.c1y, k[e], c.v[e]);
-                        an.v[e] = fmaT(a.c1a, k[e], c.v[e]);
-                    }
+                    for (int e = 0; e < 2; ++e) en.v[e] = fmaT(a.c1y, k[e], c.v[e]);
                 } else {
+                    // y3, and acc + (y3 - q)/3 (= acc + dt/3 k3) for the fourth stage
                     const V2 qv = lds2(PW + m_e8);
                     const V2 av = lds2(PW + SEBYTES + m_a8);
+                    V2 an;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         en.v[e] = fmaT(a.c1y, k[e], qv.v[e]);
-                        an.v[e] = fmaT(a.c1a, k[e], av.v[e]);
+                        an.v[e] = add_third(en.v[e], qv.v[e], av.v[e]);
                     }
+                    aw[K] = an;
                 }
                 sts2(E + m_e8, en);
                 ew[K] = en;
-                aw[K] = an;
             }
             // first stage, ring chunk
             if (has_h) {
@@ -366,17 +368,19 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
             if (v >= 4) {
                 double k[2];
                 rhs_s<WE>(a.w, E2 + m_e8, ew[(K + 3) % 5], ew[(K + 1) % 5], ew[(K + 2) % 5], ew[(K + 4) % 5], ew[K], k);
-                const V2& ap = aw[(K + 3) % 5];
                 V2 o;
                 [[maybe_unused]] V2 oa;
                 if constexpr (PAIR == 0) {
+                    // y2, and acc = q + (y1 - q)/3 + dt/3 k2
                     const V2& qc = qw[K];
+                    const V2& y1 = ew[(K + 3) % 5];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         o.v[e] = fmaT(a.c2y, k[e], qc.v[e]);
-                        oa.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
+                        oa.v[e] = fmaT(a.c2a, k[e], add_third(y1.v[e], qc.v[e], qc.v[e]));
                     }
                 } else {
+                    const V2& ap = aw[(K + 3) % 5];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) o.v[e] = fmaT(a.c2a, k[e], ap.v[e]);
                 }
@@ -529,11 +533,11 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     fill_w13<double>(a.w, L.coef, L.nu);
     const double dthalf = L.dt * .5;
     if (PAIR == 0) {  // the coefficients of stages 1 and 2 of the single-stage path
-        a.c1y = dthalf; a.c1a = L.dt / 6.; a.c2y = dthalf; a.c2a = L.dt / 3.;
+        a.c1y = dthalf; a.c2y = dthalf; a.c2a = L.dt / 3.;
         a.yout = static_cast<double*>(L.y2);
         a.aout = static_cast<double*>(L.acc);
     } else {          // stages 3 and 4
-        a.c1y = L.dt; a.c1a = L.dt / 3.; a.c2a = L.dt / 6.;
+        a.c1y = L.dt; a.c2a = L.dt / 6.;
         a.qout = static_cast<double*>(L.out);
         a.o_item_stride = go.total; a.o_origin = go.origin; a.o_px = go.px; a.o_plane = go.plane;
         a.o_halo = go.halo;

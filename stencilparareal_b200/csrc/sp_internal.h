@@ -21,10 +21,10 @@ Geo make_geo(int ni, int nj, int nk, int es, int halo = 2);
 
 // Kernel families.
 enum Op : int {
-    OP_RK_S1 = 0,  // k=R(q);  y=q+(dt/2)k;  a=q+(dt/6)k
-    OP_RK_S2 = 1,  // k=R(y);  y'=q+(dt/2)k; a+=(dt/3)k
-    OP_RK_S3 = 2,  // k=R(y);  y'=q+dt k;    a+=(dt/3)k
-    OP_RK_S4 = 3,  // k=R(y);  out=a+(dt/6)k
+    OP_RK_S1 = 0,  // k=R(q);  y1=q+(dt/2)k                               (reads q)
+    OP_RK_S2 = 1,  // k=R(y1); y2=q+(dt/2)k; a=q+(y1-q)/3+(dt/3)k         (reads y1, q)
+    OP_RK_S3 = 2,  // k=R(y2); y3=q+dt k                                  (reads y2, q)
+    OP_RK_S4 = 3,  // k=R(y3); out=a+(y3-q)/3+(dt/6)k                     (reads y3, a, q)
     OP_EULER = 4,  // k=R2(y); out=y+dt k
     OP_ADJ = 5,    // adjoint stage (see sp_adjoint.cu)
     OP_COUNT = 6

@@ -116,13 +116,13 @@ struct KArgs {
 
 template <int OP>
 struct OpTraits {
-    static constexpr int npw = (OP == OP_RK_S2 || OP == OP_RK_S3) ? 2
-                             : (OP == OP_RK_S4) ? 1
+    static constexpr int npw = (OP == OP_RK_S2 || OP == OP_RK_S3) ? 1   // q
+                             : (OP == OP_RK_S4) ? 2                        // acc, q
                              : (OP == OP_ADJ + 0) ? 1      // ADJ4: y4
                              : (OP == OP_ADJ + 1 || OP == OP_ADJ + 2) ? 3   // ADJ3/ADJ2: y, lam, lam_acc
                              : (OP == OP_ADJ + 3) ? 2      // ADJ1: y1, lam_acc
                              : 0;
-    static constexpr bool writes_a = (OP == OP_RK_S1 || OP == OP_RK_S2 || OP == OP_RK_S3 || OP == OP_ADJ + 0 ||
+    static constexpr bool writes_a = (OP == OP_RK_S2 || OP == OP_ADJ + 0 ||
                                       OP == OP_ADJ + 1 || OP == OP_ADJ + 2);
     static constexpr bool adjoint = OP >= OP_ADJ;
 };
@@ -158,14 +158,15 @@ __device__ __forceinline__ void cell_op(const KArgs<T>& a, T nl, const Nb<T>& s,
             const T k = fmaT(nl, lap, adv);
             if constexpr (OP == OP_RK_S1) {
                 oy = fmaT(a.c_y, k, s.c);
-                oa = fmaT(a.c_acc, k, s.c);
-            } else if constexpr (OP == OP_RK_S2 || OP == OP_RK_S3) {
+            } else if constexpr (OP == OP_RK_S2) {
                 oy = fmaT(a.c_y, k, p0);
-                oa = fmaT(a.c_acc, k, p1);
+                oa = fmaT(a.c_acc, k, add_third(s.c, p0, p0));
+            } else if constexpr (OP == OP_RK_S3) {
+                oy = fmaT(a.c_y, k, p0);
             } else {  // S4
-                oy = fmaT(a.c_acc, k, p0);
+                oy = fmaT(a.c_acc, k, add_third(s.c, p1, p0));
             }
-            (void)g; (void)live;
+            (void)g; (void)live; (void)p1; (void)oa;
         } else {
             // R^T m = -sum_d c_d D_d m + nu L m (D_d antisymmetric, L symmetric on the periodic grid)
             const T ybar = a.sigma * fmaT(nl, lap, -adv);
@@ -473,12 +474,13 @@ __global__ void __launch_bounds__(32 * TY)
                 const T k = rhs_w13(a.w, s);
                 if constexpr (OP == OP_RK_S1) {
                     vy = fmaT(a.c_y, k, s.c);
-                    va = fmaT(a.c_acc, k, s.c);
-                } else if constexpr (OP == OP_RK_S2 || OP == OP_RK_S3) {
+                } else if constexpr (OP == OP_RK_S2) {
                     vy = fmaT(a.c_y, k, q0);
-                    va = fmaT(a.c_acc, k, q1);
+                    va = fmaT(a.c_acc, k, add_third(s.c, q0, q0));
+                } else if constexpr (OP == OP_RK_S3) {
+                    vy = fmaT(a.c_y, k, q0);
                 } else {
-                    vy = fmaT(a.c_acc, k, q0);
+                    vy = fmaT(a.c_acc, k, add_third(s.c, q1, q0));
                 }
             } else {
                 cell_op<T, OP>(a, nl, s, q0, q1, q2, vy, va, g, live && x + e < a.ni);
@@ -570,10 +572,10 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err)
     a.err = err;
     fill_w13<T>(a.w, c, L.nu);  // RHS4 as per-offset weights (TMA RK stages; one nu per launch)
     switch (L.op) {
-        case OP_RK_S1: a.aout = (T*)L.acc; break;
-        case OP_RK_S2:
-        case OP_RK_S3: a.aout = (T*)L.acc; a.pw0 = (const T*)L.q; a.pw1 = (const T*)L.acc; break;
-        case OP_RK_S4: a.pw0 = (const T*)L.acc; break;
+        case OP_RK_S1: break;
+        case OP_RK_S2: a.aout = (T*)L.acc; a.pw0 = (const T*)L.q; break;
+        case OP_RK_S3: a.pw0 = (const T*)L.q; break;
+        case OP_RK_S4: a.pw0 = (const T*)L.acc; a.pw1 = (const T*)L.q; break;
         case OP_EULER: break;
         case OP_ADJ + 0: a.aout = (T*)L.lam_acc; a.pw0 = (const T*)L.ypt; break;
         case OP_ADJ + 1:

@@ -210,7 +210,7 @@ cudaError_t enqueue_rk4_step3(const Geo& g, int prec, const Coef& c, double dt, 
     L.op = OP_RK_S3; L.yin = yb; L.q = in; L.yout = yc; L.c_y = dt; L.c_acc = dt / 3.;
     if ((e = launch_stage(g, L, t, s, err)) != cudaSuccess) return e;
     // S4
-    L.op = OP_RK_S4; L.yin = yc; L.q = nullptr; L.yout = out; L.c_acc = dt / 6.;
+    L.op = OP_RK_S4; L.yin = yc; L.q = in; L.yout = out; L.c_acc = dt / 6.;
     return launch_stage(g, L, t, s, err);
 }
 
@@ -717,7 +717,7 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
         for (int r = 0; r < reps && e == cudaSuccess; ++r) {
             cudaEventRecord(ev[0], s);
             for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
-                L.op = op[k]; L.yin = yin[k]; L.yout = yout[k]; L.acc = ac; L.q = (k == 1 || k == 2) ? q : nullptr;
+                L.op = op[k]; L.yin = yin[k]; L.yout = yout[k]; L.acc = ac; L.q = k == 0 ? nullptr : q;
                 L.c_y = cy[k]; L.c_acc = ca[k];
                 e = launch_stage(g, L, t, s, err);
                 cudaEventRecord(ev[k + 1], s);

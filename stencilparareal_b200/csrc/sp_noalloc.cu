@@ -126,7 +126,7 @@ extern "C" int sp_do_rk4_noalloc(const sp_params* p, const double* in, double* o
         if ((e = launch_stage(g, L, t, s, ds->err)) != cudaSuccess) break;
         L.op = OP_RK_S3; L.yin = yb; L.q = src; L.yout = ya; L.c_y = dt; L.c_acc = dt / 3.;
         if ((e = launch_stage(g, L, t, s, ds->err)) != cudaSuccess) break;
-        L.op = OP_RK_S4; L.yin = ya; L.q = nullptr; L.yout = out; L.c_acc = dt / 6.;
+        L.op = OP_RK_S4; L.yin = ya; L.q = src; L.yout = out; L.c_acc = dt / 6.;
         if ((e = launch_stage(g, L, t, s, ds->err)) != cudaSuccess) break;
     }
     if (e != cudaSuccess) return sp_report(SP_ERR_CUDA, "sp_do_rk4_noalloc: launch failed: %s", cudaGetErrorString(e));

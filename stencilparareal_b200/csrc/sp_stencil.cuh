@@ -44,6 +44,15 @@ __device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
     return fmaT(w.c, s.c, (sx + sy) + sz);
 }
 
+// The accumulator terms of the low-storage RK4 step recovered from stage
+// values: dt/6 k1 = (y1 - q)/3 and dt/3 k3 = (y3 - q)/3, so that no stage
+// before the second writes the accumulator and the third neither reads nor
+// writes it.  Returns base + (y - q)/3.
+template <typename T>
+__device__ __forceinline__ T add_third(T y, T q, T base) {
+    return fmaT(y - q, T(1.0 / 3.0), base);
+}
+
 // Tensor map over `items` fields of geometry g starting at `base`: dims
 // (px, py, pz*items), box (bw, bh, 1), no swizzle, out-of-range reads as zero.
 bool make_tmap(CUtensorMap* tm, const Geo& g, const void* base, int items, int bw, int bh);
