@@ -268,6 +268,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
         //   sa[u % 5]: shared address of the slot of stencil plane u
         V2 qw[5], ew[5];
         [[maybe_unused]] V2 aw[5];  // pair 3+4 only
+        [[maybe_unused]] V2 hw[5];  // pair 1+2: the ring chunk's stencil input, like qw
         uint32_t sa[5];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {  // prologue: stencil planes 0..3
@@ -275,6 +276,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
             if (!mbar_wait_bounded(&bar[gu % NSQ], (gu / NSQ) & 1)) bad = true;
             sa[u] = s_base + (gu % NSQ) * SBYTES;
             qw[u] = lds2(sa[u] + m_s8);
+            if constexpr (PAIR == 0) hw[u] = lds2(sa[u] + h_s8);
         }
         sa[4] = 0;
 #pragma unroll
@@ -318,6 +320,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
             const uint32_t S0 = sa[K], S1 = sa[(K + 1) % 5], S2 = sa[(K + 2) % 5], S3 = sa[(K + 3) % 5],
                            S4 = sa[(K + 4) % 5];
             qw[(K + 4) % 5] = lds2(S4 + m_s8);
+            (void)S0; (void)S1; (void)S3;
             [[maybe_unused]] uint32_t PW = 0;
             if constexpr (PAIR == 1) {
                 if (!mbar_wait_bounded(&bar[NSQ + sp_v], ph_p)) bad = true;
@@ -353,9 +356,16 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
             }
             // first stage, ring chunk
             if (has_h) {
-                const V2 zm2 = lds2(S0 + h_s8), zm1 = lds2(S1 + h_s8);
-                const V2 zp1 = lds2(S3 + h_s8), zp2 = lds2(S4 + h_s8);
-                const V2 cen = lds2(S2 + h_s8);
+                V2 zm2, zm1, cen, zp1, zp2;
+                if constexpr (PAIR == 0) {  // z-window in registers (pair 1+2 has them to spare)
+                    hw[(K + 4) % 5] = lds2(S4 + h_s8);
+                    zm2 = hw[K]; zm1 = hw[(K + 1) % 5]; cen = hw[(K + 2) % 5];
+                    zp1 = hw[(K + 3) % 5]; zp2 = hw[(K + 4) % 5];
+                } else {
+                    zm2 = lds2(S0 + h_s8); zm1 = lds2(S1 + h_s8);
+                    zp1 = lds2(S3 + h_s8); zp2 = lds2(S4 + h_s8);
+                    cen = lds2(S2 + h_s8);
+                }
                 double k[2];
                 rhs_s<WB>(a.w, S2 + h_s8, cen, zm2, zm1, zp1, zp2, k);
                 V2 base = cen, hv;
