@@ -39,6 +39,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 #include <utility>
 
@@ -530,12 +531,19 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     if (total >= 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     if (sh.zchunk > 0) {
         a.span = sh.zchunk;
-    } else {  // persistent: one range per resident CTA
-        int dev = 0, sms = 0, occ = 0;
+    } else {  // persistent: one range per resident CTA (resident CTAs per device cached)
+        static std::atomic<int> cached[64];  // zero-initialised (static storage)
+        int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP>, 32 * TY, S::smem);
-        const long long ctas = std::max(1LL, (long long)std::max(1, sms) * std::max(1, occ) / a.cy);  // groups
+        int ctas_dev = (dev >= 0 && dev < 64) ? cached[dev].load(std::memory_order_relaxed) : 0;
+        if (ctas_dev == 0) {
+            int sms = 0, occ = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP>, 32 * TY, S::smem);
+            ctas_dev = std::max(1, sms) * std::max(1, occ);
+            if (dev >= 0 && dev < 64) cached[dev].store(ctas_dev, std::memory_order_relaxed);
+        }
+        const long long ctas = std::max(1LL, (long long)ctas_dev / a.cy);  // groups
         a.span = (int)std::max(1LL, (total + ctas - 1) / ctas);
     }
     a.item_lo = L.item_lo;
