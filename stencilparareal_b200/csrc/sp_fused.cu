@@ -455,23 +455,6 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
 
 
 
-// Launches a kernel with programmatic stream serialization (the kernels here
-// call pdl_trigger/pdl_wait), so that in a stream or a captured graph the
-// next kernel's CTAs start while this one's last CTAs finish.
-template <typename... KP, typename... A>
-cudaError_t launch_pdl(void (*k)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
-}
 
 // ---------------------------------------------------------------------------
 // Widening: interior of a caller-layout field -> internal field with every

@@ -345,7 +345,6 @@ __global__ void __launch_bounds__(32 * TY)
     uint64_t* bar = reinterpret_cast<uint64_t*>(ps + NP * NPA * PT);
 
     const int b = blockIdx.z;
-    if (a.item_lo && b + a.item_base < *a.item_lo) return;
     const int x0 = (blockIdx.x % a.tiles_x) * TX;
     const int y0 = (blockIdx.x / a.tiles_x) * TY;
     const int z0 = blockIdx.y * a.zchunk;
@@ -356,6 +355,7 @@ __global__ void __launch_bounds__(32 * TY)
     const int ylast = z1 + 1;     // last stencil plane needed
     const bool leader = threadIdx.x == 0;
 
+    pdl_trigger();  // the next kernel's CTAs may start as this grid's CTAs retire
     if (leader) {
         prefetch_tensormap(&tm_s);
 #pragma unroll
@@ -363,6 +363,8 @@ __global__ void __launch_bounds__(32 * TY)
         fence_mbar_init();
     }
     __syncthreads();
+    pdl_wait();     // fields written by the previous kernel are read from here on
+    if (a.item_lo && b + a.item_base < *a.item_lo) return;  // the same for all threads of the CTA
 
     // tile t (interior plane, z0-2 <= t <= z1+1) -> slot (t - z0 + 2) % NS
     auto issue_y = [&](int t) {
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(32 * TY)
         T row[3 * VX];
         {
             const T* R = Y + (w + 2) * W + lane * VX;
-            const V r0 = ld16<T>(R), r1 = ld16<T>(R + VX), r2 = ld16<T>(R + 2 * VX);
+            const V r0 = ld16<T>(R), r1 = c0, r2 = ld16<T>(R + 2 * VX);  // c0: this plane's centre
 #pragma unroll
             for (int e = 0; e < VX; ++e) { row[e] = r0.v[e]; row[VX + e] = r1.v[e]; row[2 * VX + e] = r2.v[e]; }
         }
@@ -631,8 +633,7 @@ cudaError_t launch_tma_T(const Geo& g, const StageLaunch& L, KArgs<T> a, const S
     dim3 grid(a.tiles_x * tiles_y, a.nzc, L.items);
     if (grid.y > 65535u || grid.z > 65535u) return cudaErrorInvalidConfiguration;
     const size_t smem = tma_smem_bytes<T, OP, TY, NS, NP>();
-    k_stage_tma<T, OP, TY, NS, NP><<<grid, 32 * TY, smem, s>>>(ts, t0, t1, t2, a);
-    return cudaGetLastError();
+    return launch_pdl(k_stage_tma<T, OP, TY, NS, NP>, grid, dim3(32 * TY), smem, s, ts, t0, t1, t2, a);
 }
 
 template <typename T, int OP, int TY, int NS, int NP>

@@ -4,6 +4,9 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <utility>
 
 #include "sp_device.cuh"
 #include "sp_internal.h"
@@ -51,6 +54,24 @@ __device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
 template <typename T>
 __device__ __forceinline__ T add_third(T y, T q, T base) {
     return fmaT(y - q, T(1.0 / 3.0), base);
+}
+
+// Launches a kernel with programmatic stream serialization (kernels launched
+// this way call pdl_trigger/pdl_wait), so that in a stream or a captured graph the
+// next kernel's CTAs start while this one's last CTAs finish.
+template <typename... KP, typename... A>
+cudaError_t launch_pdl(void (*k)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
 // Tensor map over `items` fields of geometry g starting at `base`: dims
