@@ -144,6 +144,19 @@ __device__ __forceinline__ Vec<double, 2> lds2o(uint32_t addr) {
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2+%3];" : "=d"(r.v[0]), "=d"(r.v[1]) : "r"(addr), "n"(OFF));
     return r;
 }
+// 16 bytes of T (2 doubles / 4 floats) by 32-bit shared address, plus OFF bytes.
+template <typename T, int OFF = 0>
+__device__ __forceinline__ Vec<T, V16<T>::N> lds16(uint32_t addr) {
+    Vec<T, V16<T>::N> r;
+    if constexpr (sizeof(T) == 8) {
+        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2+%3];" : "=d"(r.v[0]), "=d"(r.v[1]) : "r"(addr), "n"(OFF));
+    } else {
+        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];"
+                     : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3])
+                     : "r"(addr), "n"(OFF));
+    }
+    return r;
+}
 __device__ __forceinline__ void sts2(uint32_t addr, const Vec<double, 2>& v) {
     asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.v[0]), "d"(v.v[1]) : "memory");
 }

@@ -39,6 +39,7 @@
 #include <atomic>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "sp_device.cuh"
 #include "sp_internal.h"
@@ -388,14 +389,21 @@ __global__ void __launch_bounds__(32 * TY)
     }
 
     // running ring positions: slot and phase of stencil tile z+2 (the next
-    // centre), of tile z (x/y neighbours) and of pointwise tile z
+    // centre), of tile z (x/y neighbours) and of pointwise tile z.  Shared
+    // memory is read by 32-bit address with constant offsets, and the z-window
+    // of centres lives in five registers renamed statically (the plane loop is
+    // unrolled by five), so that no plane moves values between registers.
+    constexpr int ES = (int)sizeof(T);
+    const uint32_t ys_base = smem_u32(ys);
+    const uint32_t ps_base = smem_u32(ps);
+    const uint32_t own8 = (uint32_t)(((w + 2) * W + LX + lane * VX) * ES);  // this thread's centre
+    const uint32_t pw8 = (uint32_t)((w * TX + lane * VX) * ES);
     int s_c = 0;
     uint32_t ph_c = 0;
     bool bad = false;
-    const int own = (w + 2) * W + LX + lane * VX;  // this thread's centre in a stencil tile
     auto next_center = [&]() -> V {
         if (!mbar_wait_bounded(&bar[s_c], ph_c)) bad = true;
-        const V v = ld16<T>(ys + s_c * YT + own);
+        const V v = lds16<T>(ys_base + (uint32_t)s_c * YBYTES + own8);
         if (++s_c == NS) { s_c = 0; ph_c ^= 1u; }
         return v;
     };
@@ -409,7 +417,11 @@ __global__ void __launch_bounds__(32 * TY)
             (void)mbar_wait_bounded(&bar[NS + (t - z0) % NP], (uint32_t)(((t - z0) / NP) & 1));
     };
 
-    V cm2 = next_center(), cm1 = next_center(), c0 = next_center(), cp1 = next_center();
+    V cw[5];  // centres of planes z-2 .. z+2 at cw[(z - z0 + 0..4) % 5]
+    cw[0] = next_center();
+    cw[1] = next_center();
+    cw[2] = next_center();
+    cw[3] = next_center();
     if (__syncthreads_or(bad)) {
         if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
         drain(z0 + 1, z0 - 1);
@@ -425,7 +437,10 @@ __global__ void __launch_bounds__(32 * TY)
     const int x = x0 + lane * VX;
     const bool live = y < a.nj && x < a.ni;
     const bool full_vec = x + VX <= a.ni;
-    const bool img_xy = x0 < 2 || x0 + TX > a.ni - 2 || y0 < 2 || y0 + TY > a.nj - 2;
+    // rows whose cells have no y image and vectors whose cells all lie inside
+    // take the plain store (plus x images where a cell is within 2 of an x face)
+    const bool x_img = x < 2 || x + VX > a.ni - 2;
+    const bool y_img = y < 2 || y >= a.nj - 2 || !full_vec;
     const long long ob = (long long)b * a.item_stride + a.origin;
     T* yrow_out = a.yout + ob + (long long)z0 * a.plane + (long long)y * a.px + x;
     T* arow_out = nullptr;
@@ -435,29 +450,34 @@ __global__ void __launch_bounds__(32 * TY)
     int s_p = 0;
     uint32_t ph_p = 0;
 
-    for (int z = z0; z < z1; ++z) {
-        const V cp2 = next_center();
+    // one plane; K = (z - z0) % 5 names the registers of the z-window
+    auto iterate = [&](auto kc, int z) -> bool {
+        constexpr int K = decltype(kc)::value;
+        cw[(K + 4) % 5] = next_center();
+        const V& cm2 = cw[K];
+        const V& cm1 = cw[(K + 1) % 5];
+        const V& c0 = cw[(K + 2) % 5];
+        const V& cp1 = cw[(K + 3) % 5];
+        const V& cp2 = cw[(K + 4) % 5];
         V p0v, p1v, p2v;
         if constexpr (NPA > 0) {
             if (!mbar_wait_bounded(&bar[NS + s_p], ph_p)) bad = true;
-            const T* P = ps + s_p * NPA * PT + w * TX + lane * VX;
-            p0v = ld16<T>(P);
-            if constexpr (NPA > 1) p1v = ld16<T>(P + PT);
-            if constexpr (NPA > 2) p2v = ld16<T>(P + 2 * PT);
+            const uint32_t P = ps_base + (uint32_t)s_p * (uint32_t)(NPA * PT * ES) + pw8;
+            p0v = lds16<T>(P);
+            if constexpr (NPA > 1) p1v = lds16<T, PT * ES>(P);
+            if constexpr (NPA > 2) p2v = lds16<T, 2 * PT * ES>(P);
             if (++s_p == NP) { s_p = 0; ph_p ^= 1u; }
         }
-        const T* Y = ys + s_n * YT;
+        const uint32_t C = ys_base + (uint32_t)s_n * YBYTES + own8;
         if (++s_n == NS) s_n = 0;
         T row[3 * VX];
         {
-            const T* R = Y + (w + 2) * W + lane * VX;
-            const V r0 = ld16<T>(R), r1 = c0, r2 = ld16<T>(R + 2 * VX);  // c0: this plane's centre
+            const V r0 = lds16<T, -LX * ES>(C), r2 = lds16<T, VX * ES>(C);  // c0: this plane's centre
 #pragma unroll
-            for (int e = 0; e < VX; ++e) { row[e] = r0.v[e]; row[VX + e] = r1.v[e]; row[2 * VX + e] = r2.v[e]; }
+            for (int e = 0; e < VX; ++e) { row[e] = r0.v[e]; row[VX + e] = c0.v[e]; row[2 * VX + e] = r2.v[e]; }
         }
-        const T* Cn = Y + LX + lane * VX;
-        const V ym2 = ld16<T>(Cn + w * W), ym1 = ld16<T>(Cn + (w + 1) * W);
-        const V yp1 = ld16<T>(Cn + (w + 3) * W), yp2 = ld16<T>(Cn + (w + 4) * W);
+        const V ym2 = lds16<T, -2 * W * ES>(C), ym1 = lds16<T, -W * ES>(C);
+        const V yp1 = lds16<T, W * ES>(C), yp2 = lds16<T, 2 * W * ES>(C);
         V oy, oa;
 #pragma unroll
         for (int e = 0; e < VX; ++e) {
@@ -491,8 +511,18 @@ __global__ void __launch_bounds__(32 * TY)
             oa.v[e] = va;
         }
         if (live) {
-            if (!img_xy && z >= 2 && z < a.nk - 2 && full_vec) st16<T>(yrow_out, oy);
-            else store_images_vec<T, VX>(a.yout + ob, x, y, z, oy, a, true);
+            if (!y_img && z >= 2 && z < a.nk - 2) {
+                st16<T>(yrow_out, oy);
+                if (x_img) {
+#pragma unroll
+                    for (int e = 0; e < VX; ++e) {
+                        if (x + e < 2) yrow_out[e + a.ni] = oy.v[e];
+                        if (x + e >= a.ni - 2) yrow_out[e - a.ni] = oy.v[e];
+                    }
+                }
+            } else {
+                store_images_vec<T, VX>(a.yout + ob, x, y, z, oy, a, true);
+            }
             if constexpr (OpTraits<OP>::writes_a) {
                 if (full_vec) st16<T>(arow_out, oa);
                 else put_vec<T, VX>(arow_out, x, a.ni, oa);
@@ -500,11 +530,10 @@ __global__ void __launch_bounds__(32 * TY)
         }
         yrow_out += a.plane;
         if constexpr (OpTraits<OP>::writes_a) arow_out += a.plane;
-        cm2 = cm1; cm1 = c0; c0 = cp1; cp1 = cp2;
         if (__syncthreads_or(bad)) {
             if (leader) atomicExch(a.err, DEV_WAIT_TIMEOUT);
             drain(z + 2, z);
-            return;
+            return false;
         }
         if (leader) {
             fence_proxy_async_smem();
@@ -512,8 +541,15 @@ __global__ void __launch_bounds__(32 * TY)
             if constexpr (NPA > 0)
                 if (z + NP < z1) { issue_p(z + NP); p_hi = z + NP; }
         }
+        return true;
+    };
+    for (int zz = z0; zz < z1; zz += 5) {
+        if (!iterate(std::integral_constant<int, 0>{}, zz)) return;
+        if (zz + 1 < z1 && !iterate(std::integral_constant<int, 1>{}, zz + 1)) return;
+        if (zz + 2 < z1 && !iterate(std::integral_constant<int, 2>{}, zz + 2)) return;
+        if (zz + 3 < z1 && !iterate(std::integral_constant<int, 3>{}, zz + 3)) return;
+        if (zz + 4 < z1 && !iterate(std::integral_constant<int, 4>{}, zz + 4)) return;
     }
-    (void)c0;
     if constexpr (OpTraits<OP>::adjoint) reduce_par(g, a.par_acc, a.gs_nu, a.gs_c);
 }
 
