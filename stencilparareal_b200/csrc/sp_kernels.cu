@@ -487,7 +487,7 @@ __global__ void __launch_bounds__(32 * TY)
             s.xm2 = row[LX + e - 2]; s.xp2 = row[LX + e + 2];
             s.ym1 = ym1.v[e]; s.yp1 = yp1.v[e]; s.ym2 = ym2.v[e]; s.yp2 = yp2.v[e];
             s.zm1 = cm1.v[e]; s.zp1 = cp1.v[e]; s.zm2 = cm2.v[e]; s.zp2 = cp2.v[e];
-            T q0 = 0, q1 = 0, q2 = 0;
+            [[maybe_unused]] T q0 = 0, q1 = 0, q2 = 0;
             if constexpr (NPA > 0) q0 = p0v.v[e];
             if constexpr (NPA > 1) q1 = p1v.v[e];
             if constexpr (NPA > 2) q2 = p2v.v[e];

@@ -740,7 +740,8 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
 // ---------------------------------------------------------------------------
 // Autotuner: for every stage kernel (RK4 S1..S4, Euler) times each candidate
 // launch shape (kernel kind x tile rows x z-chunk) on scratch fields and keeps
-// the fastest shape per stage.
+// the fastest shape per stage; then the same for the fused stage pairs, and
+// picks fused pairs or four stage kernels per RK4 step.
 extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     int rc = check_handle(h);
     if (rc) return rc;
@@ -835,6 +836,37 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
             }
             best.fused = (pair_ms[0] + pair_ms[1]) < (op_ms[OP_RK_S1] + op_ms[OP_RK_S2] + op_ms[OP_RK_S3] +
                                                       op_ms[OP_RK_S4]) ? 1 : 0;
+            if (batch == 1) {
+                // Single fields: decide by DoRK4 itself (one graph chunk of
+                // steps), where consecutive kernels overlap through programmatic
+                // dependent launch and four stage kernels overlap more than two
+                // pairs, so that the sums of isolated kernel times mislead.
+                SP_CUDA(cudaMemsetAsync(p, 0, 2 * fb, s));
+                float path_ms[2] = {1e30f, 1e30f};
+                for (int f = 0; f < 2 && rc == SP_OK; ++f) {
+                    Tune tt = best;
+                    tt.fused = f;
+                    h->tunes[{precision, batch}] = tt;
+                    h->drop_graphs();
+                    rc = do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);  // captures the graph
+                    for (int r = 0; r < 3 && rc == SP_OK; ++r) {
+                        cudaEventRecord(e0, s);
+                        rc = do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);
+                        cudaEventRecord(e1, s);
+                        cudaEventSynchronize(e1);
+                        float m = 0;
+                        cudaEventElapsedTime(&m, e0, e1);
+                        path_ms[f] = std::min(path_ms[f], m);
+                    }
+                }
+                if (rc != SP_OK) {
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    h->drop_graphs();
+                    return rc;
+                }
+                best.fused = path_ms[1] < path_ms[0] ? 1 : 0;
+            }
         }
     }
     cudaEventDestroy(e0);
