@@ -263,7 +263,8 @@ int sp_autotune(sp_convection* h, int precision, int batch);
  * no bounded waits). */
 int sp_selftest_wait_timeout(sp_convection* h, double limit_ms);
 /* Average duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
- * events around every launch on the handle's stream over `reps` steps run on a
+ * events around every launch on the handle's stream over `reps` steps (after
+ * one untimed step; all steps enqueued before one synchronisation) run on a
  * copy of `field` (which is left unchanged).  path 0: the kernels the handle's
  * tune runs, 1: the four stage kernels (tuned shapes), 2: the fused pairs.
  * *count = 2 (ms[0..1]: pairs 1+2, 3+4) or 4 (ms[0..3]: stages S1..S4).

@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(32 * TY)
         const V& c0 = cw[(K + 2) % 5];
         const V& cp1 = cw[(K + 3) % 5];
         const V& cp2 = cw[(K + 4) % 5];
-        V p0v, p1v, p2v;
+        [[maybe_unused]] V p0v, p1v, p2v;
         if constexpr (NPA > 0) {
             if (!mbar_wait_bounded(&bar[NS + s_p], ph_p)) bad = true;
             const uint32_t P = ps_base + (uint32_t)s_p * (uint32_t)(NPA * PT * ES) + pw8;
@@ -680,7 +680,7 @@ cudaError_t set_attr_T() {
 
 template <typename T, int OP>
 cudaError_t set_attr_op() {
-    cudaError_t e = set_attr_T<T, OP, 4, 6, 3>();
+    cudaError_t e = set_attr_T<T, OP, 4, 5, 3>();
     if (e == cudaSuccess) e = set_attr_T<T, OP, 8, 5, 3>();
     if (e == cudaSuccess) e = set_attr_T<T, OP, 16, 4, 2>();
     return e;
@@ -692,7 +692,7 @@ cudaError_t set_attr_op() {
 template <typename T, int OP>
 cudaError_t launch_tma_op(const Geo& g, const StageLaunch& L, const KArgs<T>& a, const Shape& t, cudaStream_t s) {
     switch (t.ty) {
-        case 4: return launch_tma_T<T, OP, 4, 6, 3>(g, L, a, t, s);
+        case 4: return launch_tma_T<T, OP, 4, 5, 3>(g, L, a, t, s);
         case 8: return launch_tma_T<T, OP, 8, 5, 3>(g, L, a, t, s);
         case 16: return launch_tma_T<T, OP, 16, 4, 2>(g, L, a, t, s);
         default: return cudaErrorInvalidValue;

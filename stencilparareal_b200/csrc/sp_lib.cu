@@ -677,36 +677,37 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
     } else if ((rc = h->ensure_scratch(0, 2))) {  // fields 0, 3, 4, 5 of the 2-item scratch
         return rc;
     }
-    cudaEvent_t ev[5];
-    for (auto& e : ev) SP_CUDA(cudaEventCreate(&e));
+    // All launches are enqueued before one synchronisation, so that the GPU
+    // never waits for the host between them; rep 0 is an untimed warm-up.  An
+    // event between two kernels keeps them from overlapping, so each launch is
+    // timed alone.
+    const int nk = fused ? 2 : 4;
+    const int nrep = reps + 1;
+    std::vector<cudaEvent_t> ev((size_t)nrep * nk + 1, nullptr);
     cudaError_t e = cudaSuccess;
+    for (auto& x : ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&x);
     if (fused) {
-        e = launch_widen(h->g4, h->wbuf(0, 1), g, field, 1, nullptr, 0, s);
+        if (e == cudaSuccess) e = launch_widen(h->g4, h->wbuf(0, 1), g, field, 1, nullptr, 0, s);
         PairLaunch L;
         L.nu = nu; L.dt = dt; L.coef = h->coef;
-        for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
+        for (int r = 0; r < nrep && e == cudaSuccess; ++r) {
             void* Q = h->wbuf(r % 2, 1);
             void* A = h->wbuf((r + 1) % 2, 1);
             L.pair = 0; L.q = Q; L.y2 = h->wbuf(2, 1); L.acc = A; L.out = A;
-            cudaEventRecord(ev[0], s);
             e = launch_pair(h->g4, h->g4, L, t.pair[0], s, err);
-            cudaEventRecord(ev[1], s);
+            cudaEventRecord(ev[(size_t)r * 2 + 1], s);
             L.pair = 1;
             if (e == cudaSuccess) e = launch_pair(h->g4, h->g4, L, t.pair[1], s, err);
-            cudaEventRecord(ev[2], s);
-            cudaEventSynchronize(ev[2]);
-            float m0 = 0, m1 = 0;
-            cudaEventElapsedTime(&m0, ev[0], ev[1]);
-            cudaEventElapsedTime(&m1, ev[1], ev[2]);
-            acc[0] += m0; acc[1] += m1;
+            cudaEventRecord(ev[(size_t)r * 2 + 2], s);
         }
-        *count = 2;
     } else {
         void* q = h->sbuf(0, 3, 1);
         void* ya = h->sbuf(0, 4, 1);
         void* yb = h->sbuf(0, 5, 1);
         void* ac = h->sbuf(0, 0, 1);
-        e = cudaMemcpyAsync(q, field, g.total * g.es, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(q, field, g.total * g.es, cudaMemcpyDeviceToDevice, s);
         StageLaunch L;
         L.prec = 0; L.items = 1; L.nu = nu; L.coef = h->coef;
         const double dthalf = dt * .5;
@@ -714,24 +715,26 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
         const void* yin[4] = {q, ya, yb, ya};
         void* yout[4] = {ya, yb, ya, q};
         const double cy[4] = {dthalf, dthalf, dt, 0.}, ca[4] = {dt / 6., dt / 3., dt / 3., dt / 6.};
-        for (int r = 0; r < reps && e == cudaSuccess; ++r) {
-            cudaEventRecord(ev[0], s);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
+        for (int r = 0; r < nrep && e == cudaSuccess; ++r) {
             for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
                 L.op = op[k]; L.yin = yin[k]; L.yout = yout[k]; L.acc = ac; L.q = k == 0 ? nullptr : q;
                 L.c_y = cy[k]; L.c_acc = ca[k];
                 e = launch_stage(g, L, t, s, err);
-                cudaEventRecord(ev[k + 1], s);
-            }
-            cudaEventSynchronize(ev[4]);
-            for (int k = 0; k < 4; ++k) {
-                float m = 0;
-                cudaEventElapsedTime(&m, ev[k], ev[k + 1]);
-                acc[k] += m;
+                cudaEventRecord(ev[(size_t)r * 4 + k + 1], s);
             }
         }
-        *count = 4;
     }
-    for (auto& x : ev) cudaEventDestroy(x);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev.back());
+    for (int r = 1; r < nrep && e == cudaSuccess; ++r)
+        for (int k = 0; k < nk; ++k) {
+            float m = 0;
+            cudaEventElapsedTime(&m, ev[(size_t)r * nk + k], ev[(size_t)r * nk + k + 1]);
+            acc[k] += m;
+        }
+    *count = nk;
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, "kernel timing: %s", cudaGetErrorString(e));
     for (int k = 0; k < *count; ++k) ms[k] = acc[k] / reps;
     return sp_convection_synchronize(h);
