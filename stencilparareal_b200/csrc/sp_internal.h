@@ -41,7 +41,7 @@ struct Shape {
 constexpr int kNumOps = OP_ADJ + 4;
 struct Tune {
     Shape op[kNumOps];
-    Shape pair[2];    // fused stage pairs 1+2 and 3+4 (ty 8 or 16)
+    Shape pair[2] = {Shape{8, 0, 1}, Shape{8, 0, 1}};  // fused stage pairs 1+2 and 3+4 (ty 8 or 16)
     int fused = 0;    // 1: FP64 RK4 steps run as the two fused pairs
     void set_all(const Shape& s) {
         for (auto& o : op) o = s;

@@ -159,4 +159,8 @@ def test_kernel_times_paths_leave_field_unchanged(sp):
     assert set(kp) == {"P12", "P34"} and set(kt) == {"P12", "P34"}
     assert set(ks) == {"S1", "S2", "S3", "S4"}
     assert all(v > 0 for v in list(kp.values()) + list(ks.values()))
+    # a single-stage tune keeps valid pair shapes for timing the pairs
+    c.set_tune(sp.SP_F64, 1, 4, 8, 1)
+    kp2 = c.kernel_times(f, 1e-4, reps=2, path="pairs")
+    assert set(kp2) == {"P12", "P34"} and all(v > 0 for v in kp2.values())
     assert torch.equal(f.data, before)
