@@ -174,10 +174,10 @@ def cpu_baseline_sample():
             "sample": f"{steps} RK4 steps of {n}^3 (oracle restating the reference OpenMP path), {dt:.1f} s"}
 
 
-def cpu_config_times(torch, sp, device, gpu_c3_serial_s=None):
-    """CPU (oracle, all host cores) beside GPU times for config 1 in full (32^3, 1000 RK4
-    steps) and for config 3's serial fine propagator (128^3, 20000 steps; CPU on 200
-    steps, extrapolated)."""
+def cpu_vs_gpu_times(torch, sp, device, gpu_serial_128_s=None):
+    """CPU (oracle, all host cores) beside GPU times for the 32^3 serial fine run in full
+    (1000 RK4 steps) and for the 128^3 serial fine propagator of the Parareal workload
+    (20000 steps; CPU on 200 steps, extrapolated)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     from oracle import oracle as O
@@ -199,20 +199,22 @@ def cpu_config_times(torch, sp, device, gpu_c3_serial_s=None):
     conv.DoRK4(fi, fo, 0.0, dt, steps)
     conv.synchronize()
     gpu = time.perf_counter() - t0
-    out["config1"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01", "cpu_s": cpu, "gpu_s": gpu}
+    out["serial_fine_32cube_1000_steps"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01", "cpu_s": cpu, "gpu_s": gpu}
     n, sample, total = 128, 200, 20000
     p = O.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
     q0 = gaussian_noise(n, seed=0)
     t0 = time.perf_counter()
     O.rk4(p, q0, 0.0, 1e-5, sample)
     cpu = time.perf_counter() - t0
-    out["config3_serial_fine"] = {"what": "128^3, 20000 RK4 FP64 steps, dt=1e-5", "cpu_s_extrapolated": cpu * total / sample,
-                                  "cpu_sample": f"{sample} of {total} steps in {cpu:.2f} s", "gpu_s": gpu_c3_serial_s}
+    out["serial_fine_128cube_20000_steps"] = {"what": "128^3, 20000 RK4 FP64 steps, dt=1e-5",
+                                              "cpu_s_extrapolated": cpu * total / sample,
+                                              "cpu_sample": f"{sample} of {total} steps in {cpu:.2f} s",
+                                              "gpu_s": gpu_serial_128_s}
     return out
 
 
 def parareal_summary(torch, sp, device):
-    """Config 3: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice)."""
+    """Parareal on one GPU: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     n, P, T = 128, 32, 0.2
@@ -251,7 +253,7 @@ def parareal_summary(torch, sp, device):
 
 
 def batch_summary(torch, sp, device, n_inst=48, seed=2):
-    """Config 4: 48 independent Parareal solves, grids drawn from {32,48,64,96}^3, nu log-uniform in
+    """Batched uneven instances: 48 independent Parareal solves, grids drawn from {32,48,64,96}^3, nu log-uniform in
     [1e-4, 1e-2], c uniform in [-1,1]^3, 8-24 slices; T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32
     dt=1e-3 (totals rounded up to a multiple of the slice count), tolerance 1e-8 relative L2 against
     each instance's serial FP64 fine solution."""
@@ -309,7 +311,7 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
 
 
 def adjoint_summary(torch, sp, device):
-    """Config 5: gradient of 0.5||q(T)-q_target||^2 through 400 RK4 FP64 steps at 128^3, checkpoint 20."""
+    """Adjoint: gradient of 0.5||q(T)-q_target||^2 through 400 RK4 FP64 steps at 128^3, checkpoint 20."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     from stencilparareal_b200.adjoint import misfit_gradient
@@ -503,10 +505,10 @@ def main():
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample()
             try:
-                line["cpu_configs"] = cpu_config_times(torch, sp, device,
-                                                       line.get("parareal", {}).get("serial_fine_s"))
+                line["cpu_vs_gpu"] = cpu_vs_gpu_times(torch, sp, device,
+                                                      line.get("parareal", {}).get("serial_fine_s"))
             except Exception as ex:  # reported, not hidden
-                line["cpu_configs"] = {"error": repr(ex)}
+                line["cpu_vs_gpu"] = {"error": repr(ex)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

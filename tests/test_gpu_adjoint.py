@@ -100,7 +100,7 @@ def test_autograd_function(sp):
     np.testing.assert_allclose(params.grad.numpy(), gp, rtol=1e-12, atol=0)
 
 
-def test_config5_adjoint_128cube_400_steps(sp):
+def test_adjoint_128cube_400_steps_vs_central_differences(sp):
     """Gradient of 0.5||q(T)-q_target||^2 wrt q0, nu, c through 400 RK4 FP64 steps (dt=5e-5) at 128^3,
     checkpoint every 20 steps, against central differences on 16 random unit directions in (q0, nu, c).
 
@@ -134,7 +134,7 @@ def test_config5_adjoint_128cube_400_steps(sp):
         fd4 = central_difference(sp, n, q0, qt, pars, dq, dp, 1e-4, dt, steps)
         worst_norm = max(worst_norm, abs(fd6 - ad) / gnorm)
         worst_rel = max(worst_rel, abs(fd4 - ad) / abs(fd4))
-    print(f"config5: J={J:.6e} |grad|={gnorm:.4e}; h=1e-6: max |fd-ad|/|grad| = {worst_norm:.3e}; "
+    print(f"adjoint 128^3: J={J:.6e} |grad|={gnorm:.4e}; h=1e-6: max |fd-ad|/|grad| = {worst_norm:.3e}; "
           f"h=1e-4: max |fd-ad|/|fd| = {worst_rel:.3e}")
     assert worst_norm < 1e-6, worst_norm
     assert worst_rel < 1e-6, worst_rel

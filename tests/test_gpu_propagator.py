@@ -76,7 +76,7 @@ def test_fp32_coarse_parity(sp, orc, n):
     assert rel_l2(c.download(fout), ref) < TOL32
 
 
-def test_config1_serial_fine_32cube_1000_steps(sp, orc):
+def test_serial_fine_32cube_1000_steps(sp, orc):
     """Serial fine propagator, FP64, 32^3, c=(1,1,1), nu=0.01, Gaussian + noise, dt=1e-4, 1000 steps."""
     n = (32, 32, 32)
     c, args = make(sp, n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
