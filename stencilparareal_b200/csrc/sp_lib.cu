@@ -800,7 +800,7 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
         op_ms[op] = best_ms;
     }
     // fused stage pairs (FP64): best shape per pair, then fused or single-stage
-    // steps by the sum of their kernel times
+    // steps by timing whole steps of both paths
     best.fused = 0;
     if (precision == SP_F64 && pair_supported(h->g4)) {
         const Geo& g4 = h->g4;
@@ -867,6 +867,52 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                     cudaEventDestroy(e1);
                     h->drop_graphs();
                     return rc;
+                }
+                best.fused = path_ms[1] < path_ms[0] ? 1 : 0;
+            } else {
+                // Batches (the Parareal F sweep): four consecutive batched steps of
+                // each path as the sweep launches them, after one untimed step.
+                SP_CUDA(cudaMemsetAsync(p, 0, 4 * fb, s));
+                SP_CUDA(cudaMemsetAsync(w, 0, 3 * wb, s));
+                const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
+                int* err = h->err.as<int>();
+                Tune ts = best;
+                ts.fused = 0;
+                auto stage_steps = [&](int k) {
+                    cudaError_t x = cudaSuccess;
+                    for (int i = 0; i < k && x == cudaSuccess; ++i)
+                        x = enqueue_rk4_step(g, precision, h->coef, 1e-9, NuSrc{nu, nullptr}, p, p, p + fb,
+                                             p + 2 * fb, p + 3 * fb, batch, nullptr, 0, ts, s, err);
+                    return x;
+                };
+                auto pair_steps = [&](int k) {
+                    cudaError_t x = cudaSuccess;
+                    for (int i = 0; i < k && x == cudaSuccess; ++i) {
+                        char* Q = w + (size_t)(i % 2) * wb;
+                        char* A = w + (size_t)((i + 1) % 2) * wb;
+                        x = enqueue_pair_step(h, best, 1e-9, nu, Q, A, w + 2 * wb, A, h->g4, batch, nullptr, 0, s,
+                                              err);
+                    }
+                    return x;
+                };
+                float path_ms[2] = {1e30f, 1e30f};
+                cudaError_t x = cudaSuccess;
+                for (int f = 0; f < 2 && x == cudaSuccess; ++f) {
+                    x = f ? pair_steps(1) : stage_steps(1);
+                    for (int r = 0; r < 3 && x == cudaSuccess; ++r) {
+                        cudaEventRecord(e0, s);
+                        x = f ? pair_steps(4) : stage_steps(4);
+                        cudaEventRecord(e1, s);
+                        cudaEventSynchronize(e1);
+                        float m = 0;
+                        cudaEventElapsedTime(&m, e0, e1);
+                        path_ms[f] = std::min(path_ms[f], m);
+                    }
+                }
+                if (x != cudaSuccess) {
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    return fail(SP_ERR_CUDA, "tuning batched steps: %s", cudaGetErrorString(x));
                 }
                 best.fused = path_ms[1] < path_ms[0] ? 1 : 0;
             }
