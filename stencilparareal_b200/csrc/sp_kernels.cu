@@ -99,6 +99,7 @@ struct KArgs {
     long long item_stride, origin, px, plane;
     int ni, nj, nk, pz;
     int tiles_x, zchunk, nzc;
+    int zrev;         // TMA kernel: CTAs take items and z-chunks in descending order
     const int* item_lo;
     int item_base;
     T ca0, ca1, ca2;          // c_d/(12dx)
@@ -345,10 +346,12 @@ __global__ void __launch_bounds__(32 * TY)
     T* ps = ys + NS * YT;
     uint64_t* bar = reinterpret_cast<uint64_t*>(ps + NP * NPA * PT);
 
-    const int b = blockIdx.z;
+    // zrev: items and z-chunks in descending order, so that a launch starts on
+    // the planes the previous launch (ascending) touched last, still in L2
+    const int b = a.zrev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z;
     const int x0 = (blockIdx.x % a.tiles_x) * TX;
     const int y0 = (blockIdx.x / a.tiles_x) * TY;
-    const int z0 = blockIdx.y * a.zchunk;
+    const int z0 = (a.zrev ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y) * a.zchunk;
     const int z1 = min(z0 + a.zchunk, a.nk);
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -608,6 +611,9 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err)
     a.lap_scale = (L.op == OP_EULER) ? c.s2 : c.s4;
     a.c_y = (T)L.c_y; a.c_acc = (T)L.c_acc;
     a.err = err;
+    // RK4 stages alternate the sweep direction (S1, S3 descending; S2, S4 ascending),
+    // so that each stage starts on the planes the previous one touched last
+    a.zrev = (L.op == OP_RK_S1 || L.op == OP_RK_S3) ? 1 : 0;
     fill_w13<T>(a.w, c, L.nu);  // RHS4 as per-offset weights (TMA RK stages; one nu per launch)
     switch (L.op) {
         case OP_RK_S1: break;
