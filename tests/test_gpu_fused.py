@@ -147,6 +147,34 @@ def test_parareal_fine_sweep_fused_equals_single_stage(sp, skip):
     assert np.array_equal(outs[0], outs[1])
 
 
+def test_batch_autotune_then_parareal_equals_single_stage(sp):
+    """The tuner's batched-step choice (fused pairs or stage kernels, by timing
+    four batched steps of each) leaves the Parareal fields bit for bit unchanged."""
+    n, P = 24, 4
+    outs = []
+    bitwise = True
+    for tune in ("auto", SINGLE):
+        conv = sp.Convection(n, n, n, 1.0 / n, 0.05, 0.0, 1.0, 0.5, -0.25)
+        if tune == "auto":
+            cfg = conv.autotune(sp.SP_F64, P)
+            assert cfg["P12"]["kind"] in (0, 2) and cfg["P12"]["ty"] in (8, 16)
+            # direct-load stage kernels evaluate R in the difference form: not bit for bit
+            bitwise = cfg["P12"]["kind"] == 2 or all(cfg[k]["kind"] == 1 for k in ("S1", "S2", "S3", "S4"))
+        else:
+            conv.set_tune(sp.SP_F64, P, *tune)
+        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.02, timeStepsFine=120,
+                                       timeStepsCoarse=12, kmax=2)
+        fin, fsol = conv.field(), conv.field()
+        conv.upload(fin, gaussian_noise(n, seed=13))
+        par = sp.Parareal(conv, fin, fsol, 0.0, conf, coarse="rk4", coarse_precision="f64")
+        par.DoParallel()
+        outs.append(conv.download(fsol))
+    if bitwise:
+        assert np.array_equal(outs[0], outs[1])
+    else:
+        assert rel_l2(outs[0], outs[1]) < 1e-13
+
+
 def test_kernel_times_paths_leave_field_unchanged(sp):
     n = (32, 32, 32)
     c = make(sp, n)
