@@ -6,17 +6,21 @@
 //
 //   reference (Convection.cpp:318-370), per RK4 step:
 //     4 x [Periodicity I/J/K kernels + RHS4 stencil] + 3 x Euler + 1 x RK
-//   here, per RK4 step (q = step start, y = stage input, a = accumulator):
-//     S1: k=R(q);  y2=q+dt/2 k;  a=q+dt/6 k
-//     S2: k=R(y2); y3=q+dt/2 k;  a+=dt/3 k
-//     S3: k=R(y3); y4=q+dt k;    a+=dt/3 k
-//     S4: k=R(y4); q+=a+dt/6 k           (16 field accesses per cell-update)
+//   here, per RK4 step (q = step start, y = stage values, a = accumulator):
+//     S1: k=R(q);  y1=q+dt/2 k
+//     S2: k=R(y1); y2=q+dt/2 k;  a=q+(y1-q)/3+dt/3 k
+//     S3: k=R(y2); y3=q+dt k
+//     S4: k=R(y3); q'=a+(y3-q)/3+dt/6 k   (13 field accesses per cell-update)
+//   ((y1-q)/3 = dt/6 k1 and (y3-q)/3 = dt/3 k3 recover two accumulator terms
+//   from stage values, so that only S2 writes the accumulator)
 //
 // R is RHS4Stage (Convection.cpp:57-82): Advection4 (ConvectionFunctions.h:66-104)
 // plus nu * Laplace4 (ConvectionFunctions.h:135-167), written as
 //   R = sum_d c_d/(12dx) * (8(q[-1]-q[+1]) - (q[-2]-q[+2]))_d
 //     + nu/(12dx^2) * (16 S1 - S2 - 90 q),  S1/S2 = sums of the +-1/+-2 neighbours,
-// the same coefficients regrouped into differences.  R2 is RHS2Stage
+// the same coefficients regrouped into differences (the direct-load kernel and
+// the adjoint); the TMA RK stages use them combined into 13 per-offset weights
+// (rhs_w13, sp_stencil.cuh), as the fused stage pairs do.  R2 is RHS2Stage
 // (Convection.cpp:30-55) with the upwind Advection2 (ConvectionFunctions.h:18-42).
 //
 // Fields carry a 2-cell halo (layout in include/sp_abi.h).  Every kernel that
