@@ -1,8 +1,8 @@
 // sp_fused.cu -- RK4 stages fused in pairs through shared memory.
 //
 // One low-storage RK4 step (src/Convection/Convection.cpp:286-327) is four
-// stencil stages.  Run one by one they move 16 field values per cell through
-// HBM (128 B in FP64).  Here stages 1+2 and stages 3+4 each run as one kernel:
+// stencil stages.  Run one by one (sp_kernels.cu) they move 13 field values per
+// cell through HBM (104 B in FP64).  Here stages 1+2 and stages 3+4 each run as one kernel:
 // the first stage of a pair is evaluated on the CTA tile widened by the
 // stencil radius (2 cells in x and y, 2 planes ahead in z) and kept in shared
 // memory, where the second stage reads it.  Per step the pairs move 7 values
