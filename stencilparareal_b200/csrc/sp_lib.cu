@@ -38,7 +38,7 @@ int fail(int code, const char* fmt, ...) {
     do {                                                                                                \
         cudaError_t e_ = (call);                                                                        \
         if (e_ != cudaSuccess) return fail(SP_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                                           "sp_lib.cu", __LINE__);                                         \
+                                           "sp_lib.cu", __LINE__);                                      \
     } while (0)
 
 // computenu (Convection.h:81-84)
