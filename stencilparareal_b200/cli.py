@@ -12,6 +12,12 @@
         reference takes from the MPI communicator size, is --timeSlices; all slices
         run on one GPU.  Energy comes from NVML (the reference reads Cray counters).
 
+    python -m stencilparareal_b200.cli findstable [--nu0 X --gridSize N --endTime T --order 1|4
+                                                   --nufreqs 100,10,1 --minSteps N --maxSteps N]
+        jobs/finalJobs/FindStable.sbatch: the convection driver over nufreq x timeSteps
+        (doubling from minSteps to maxSteps), one table row per run with the maximum
+        absolute and the relative error against the analytic solution.
+
     --mat writes the reference's MAT-v5 files into the working directory.
 """
 from __future__ import annotations
@@ -118,9 +124,11 @@ def run_convection(argv, out=sys.stdout) -> dict:
     print(f"Grid: {n}^3, timesteps: {c['timesteps']}, dt: {c['dt']:g}, CFL: {c['cfl']:g}, "
           f"order: {4 if c['rk'] else 1}", file=out)
     print(f"Timing results:\n - total time: {elapsed * 1e3:.3f} msec\n", file=out)
-    print(f"Errors: exact={x_inf:g}, error={e_inf:g}", file=out)
+    # the lines src/Convection/main.cpp:378-389 prints (one process), which
+    # jobs/finalJobs/FindStable.sbatch:29-30 parses
+    print(f"Errors on all processes:\n - Process 0 has exact={x_inf:g}, error={e_inf:g}", file=out)
     print(f"\n Total relative error: {rel:g}", file=out)
-    return dict(c, error=rel, seconds=elapsed)
+    return dict(c, error=rel, abs_error=e_inf, seconds=elapsed)
 
 
 def parareal_config(argv):
@@ -231,13 +239,55 @@ def run_parareal(argv, out=sys.stdout) -> dict:
     return res
 
 
+def findstable_config(argv):
+    """Options of jobs/finalJobs/FindStable.sbatch:4-20 (nu0 0.1, 128^3, T 0.1, order 4,
+    nufreq in {100, 10, 1}, timeSteps doubling from 1024 to 8192)."""
+    ap = argparse.ArgumentParser(prog="findstable")
+    ap.add_argument("--nu0", type=float, default=0.1)
+    ap.add_argument("--gridSize", type=int, default=128)
+    ap.add_argument("--endTime", type=float, default=0.1)
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--nufreqs", default="100,10,1")
+    ap.add_argument("--minSteps", type=int, default=1024)
+    ap.add_argument("--maxSteps", type=int, default=8192)
+    a = ap.parse_args(argv)
+    if a.minSteps < 1 or a.maxSteps < a.minSteps:
+        raise SystemExit("need 1 <= minSteps <= maxSteps")
+    steps, s = [], a.minSteps
+    while s <= a.maxSteps:
+        steps.append(s)
+        s *= 2
+    return dict(nu0=a.nu0, gridsize=a.gridSize, endtime=a.endTime, order=a.order,
+                nufreqs=[float(v) for v in a.nufreqs.split(",") if v], steps=steps)
+
+
+def run_findstable(argv, out=sys.stdout) -> list:
+    """One convection run per (nufreq, timeSteps); prints the sweep's table
+    (FindStable.sbatch:10,29-34: "Order freq tSteps AbsErr RelErr")."""
+    import io
+    c = findstable_config(argv)
+    print("Order freq tSteps    AbsErr          RelErr", file=out)
+    rows = []
+    for f in c["nufreqs"]:
+        for n_steps in c["steps"]:
+            r = run_convection(["--nu0", str(c["nu0"]), "--nufreq", str(f), "--gridSize", str(c["gridsize"]),
+                                "--endTime", str(c["endtime"]), "--timeSteps", str(n_steps),
+                                "--order", str(c["order"])], out=io.StringIO())
+            row = (c["order"], f, n_steps, r["abs_error"], r["error"])
+            rows.append(row)
+            print("%5d %4d %6d %.7e %.7e" % (row[0], int(row[1]), row[2], row[3], row[4]), file=out)
+    return rows
+
+
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
-    if not argv or argv[0] not in ("convection", "parareal"):
+    if not argv or argv[0] not in ("convection", "parareal", "findstable"):
         print(__doc__)
         return 2
     if argv[0] == "convection":
         run_convection(argv[1:])
+    elif argv[0] == "findstable":
+        run_findstable(argv[1:])
     else:
         run_parareal(argv[1:])
     return 0

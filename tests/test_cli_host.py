@@ -2,7 +2,7 @@
 import numpy as np
 
 from stencilparareal_b200 import solution as S
-from stencilparareal_b200.cli import convection_config, parareal_config
+from stencilparareal_b200.cli import convection_config, findstable_config, parareal_config
 
 
 def test_fill_q_matches_oracle(orc):
@@ -63,3 +63,13 @@ def test_matfile_roundtrip(tmp_path):
     cell = d["series"]
     assert cell.shape == (1, 2)
     np.testing.assert_array_equal(cell[0, 1], b.transpose(2, 1, 0))
+
+
+def test_findstable_options():
+    # jobs/finalJobs/FindStable.sbatch:4-20: nu0 0.1, 128^3, T 0.1, order 4,
+    # nufreq 100, 10, 1 and timeSteps 1024 doubling while <= 8192
+    c = findstable_config([])
+    assert (c["nu0"], c["gridsize"], c["endtime"], c["order"]) == (0.1, 128, 0.1, 4)
+    assert c["nufreqs"] == [100.0, 10.0, 1.0] and c["steps"] == [1024, 2048, 4096, 8192]
+    c = findstable_config(["--minSteps", "100", "--maxSteps", "450", "--nufreqs", "5"])
+    assert c["steps"] == [100, 200, 400] and c["nufreqs"] == [5.0]

@@ -19,6 +19,36 @@ def test_convection_cli_converges_at_fourth_order():
     assert 3.7 < order < 4.3, (errs, order)
 
 
+def test_findstable_sweep_table():
+    """A reduced FindStable sweep (jobs/finalJobs/FindStable.sbatch): one row per
+    (nufreq, timeSteps) with the convection driver's absolute and relative errors,
+    in the table format the script prints; the convection output carries the
+    lines the script parses."""
+    import re
+    from stencilparareal_b200.cli import run_convection, run_findstable
+    out = io.StringIO()
+    rows = run_findstable(["--gridSize", "24", "--endTime", "0.01", "--nufreqs", "100,1", "--minSteps", "50",
+                           "--maxSteps", "200"], out=out)
+    lines = out.getvalue().splitlines()
+    assert lines[0].split() == ["Order", "freq", "tSteps", "AbsErr", "RelErr"]
+    assert [(r[1], r[2]) for r in rows] == [(100.0, 50), (100.0, 100), (100.0, 200), (1.0, 50), (1.0, 100),
+                                             (1.0, 200)]
+    for line, r in zip(lines[1:], rows):
+        f = line.split()
+        assert (int(f[0]), int(f[1]), int(f[2])) == (4, int(r[1]), r[2])
+        assert abs(float(f[3]) - r[3]) <= 1e-7 * r[3] and abs(float(f[4]) - r[4]) <= 1e-7 * r[4]
+        assert 0 < r[4] < 1e-2  # stable at every step count of the sweep
+    conv_out = io.StringIO()
+    r = run_convection(["--gridSize", "24", "--endTime", "0.01", "--timeSteps", "50", "--nufreq", "100"],
+                       out=conv_out)
+    text = conv_out.getvalue()
+    err = re.search(r"^ - Process .* error=(.*)$", text, re.M)
+    rel = re.search(r"^ Total relative error: (.*)$", text, re.M)
+    assert err and rel
+    assert abs(float(err.group(1)) - r["abs_error"]) <= 1e-5 * r["abs_error"]
+    assert abs(float(rel.group(1)) - r["error"]) <= 1e-5 * r["error"]
+
+
 def test_parareal_cli_compare_mode_matches_oracle(orc):
     from stencilparareal_b200.cli import run_parareal
     out = io.StringIO()
