@@ -186,3 +186,28 @@ def test_batch_of_uneven_instances_equals_individual_runs(sp, orc):
         qo, qs, em, el = orc.parareal(orc.params(n, nu0=nu0, cx=c[0], cy=c[1], cz=c[2]), cfg, q0)
         assert rel_l2(conv.download(fb), qo) < (1e-11 if prec == "f64" else 1e-8)
         assert abs(rep["err_l2"][-1] - el[-1]) <= 1e-3 * el[-1] + 1e-12
+
+
+def test_nonfinite_defect_is_reported_and_handle_recovers(sp):
+    """Failure detection without a GPU fault: a fine step far beyond RK4's stability
+    limit (diffusion number 4, growth ~7e5 per step: the fields overflow to Inf/NaN
+    within the first slice) makes DoParallel return SP_ERR_NONFINITE instead of a result; the
+    same propagator handle then runs a stable Parareal bit for bit like a fresh one."""
+    n, P = 16, 4
+    conv = sp.Convection(n, n, n, 1.0 / n, 1.0, 0.0, 1.0, 1.0, 1.0)
+    fin, fsol = conv.field(), conv.field()
+    conv.upload(fin, gaussian_noise(n, seed=31))
+    bad = sp.RuntimeConfiguration(timeSlices=P, nu0=1.0, gridSize=n, endTime=4.0, timeStepsFine=256,
+                                  timeStepsCoarse=8, kmax=2)
+    with pytest.raises(sp.SpError) as ex:
+        sp.Parareal(conv, fin, fsol, 0.0, bad, coarse="rk4", coarse_precision="f64").DoParallel()
+    assert ex.value.code == sp._lib.SP_ERR_NONFINITE
+    good = sp.RuntimeConfiguration(timeSlices=P, nu0=1.0, gridSize=n, endTime=0.002, timeStepsFine=64,
+                                   timeStepsCoarse=8, kmax=2)
+    sp.Parareal(conv, fin, fsol, 0.0, good, coarse="rk4", coarse_precision="f64").DoParallel()
+    got = conv.download(fsol)
+    conv2 = sp.Convection(n, n, n, 1.0 / n, 1.0, 0.0, 1.0, 1.0, 1.0)
+    f2, s2 = conv2.field(), conv2.field()
+    conv2.upload(f2, gaussian_noise(n, seed=31))
+    sp.Parareal(conv2, f2, s2, 0.0, good, coarse="rk4", coarse_precision="f64").DoParallel()
+    assert np.array_equal(got, conv2.download(s2))
