@@ -14,10 +14,24 @@
 #include <tuple>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sp_abi.h"
 #include "sp_internal.h"
 
 using namespace sp;
+
+namespace {
+// Host-side NVTX range over a phase of the driver (propagation calls, the
+// Parareal predictor and iterations, the adjoint); the header-only NVTX v3
+// records nothing unless a profiler that collects NVTX is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // Errors.
@@ -335,6 +349,7 @@ constexpr int kChunk = 50;  // RK4 steps per captured graph
 
 // Convection::DoRK4 / DoEuler on single fields of precision prec.
 int do_prop(sp_convection* h, int prec, bool rk, const void* in, void* out, double tStart, double dt, int n) {
+    NvtxRange range(rk ? "Convection::DoRK4" : "Convection::DoEuler");
     int rc = check_handle(h);
     if (rc) return rc;
     if (!in || !out) return fail(SP_ERR_INVALID, "null field");
@@ -1242,6 +1257,7 @@ int sp_parareal_destroy(sp_parareal* pr) {
 }
 
 int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution) {
+    NvtxRange range("Parareal::DoSerial");
     if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
     // Parareal::DoSerial (Parareal.h:250-253)
     return sp_do_rk4(pr->prop, initial, solution, 0., pr->dtF, pr->tsF * pr->Pglobal);
@@ -1268,14 +1284,21 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     }
     if (!pr->iter && (rc = build_iteration_graph(pr))) return rc;
 
+    NvtxRange range("Parareal::DoParallel");
     SP_CUDA(cudaEventRecord(pr->ev[3], s));
-    if ((rc = enqueue_predictor(pr, initial, s))) return rc;
+    {
+        NvtxRange pred("predictor");
+        if ((rc = enqueue_predictor(pr, initial, s))) return rc;
+    }
     // Iterations (Parareal.h:116-165).
     int k = 0;
     double t_f = 0., t_c = 0.;
     long long fine_cu = 0;
     const long long cells = (long long)g.ni * g.nj * g.nk;
     for (; k < pr->cfg.kmax; ++k) {
+        char label[32];
+        std::snprintf(label, sizeof label, "iteration %d", k + 1);
+        NvtxRange it(label);
         const int lo = pr->cfg.skip_converged ? std::min(k, P) : 0;
         *pr->h_itemlo = lo;
         SP_CUDA(cudaMemcpyAsync(pr->itemlo(), pr->h_itemlo, sizeof(int), cudaMemcpyHostToDevice, s));
@@ -1352,6 +1375,7 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
 extern "C" int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* q_target, const double* lambda_n,
                               double tStart, double dt, int n, int ck, double* J, double* grad_q0,
                               double* grad_par) {
+    NvtxRange range("adjoint RK4");
     int rc = check_handle(h);
     if (rc) return rc;
     if (!q0 || !grad_q0 || (!q_target && !lambda_n)) return fail(SP_ERR_INVALID, "null field");
@@ -1530,6 +1554,7 @@ extern "C" int sp_parareal_batch_destroy(sp_parareal_batch* b) {
 extern "C" int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* initial, double* const* solution,
                                      const double* const* reference, sp_parareal_report* reports,
                                      double* seconds) {
+    NvtxRange range("PararealBatch::run");
     if (!b || !initial || !solution) return fail(SP_ERR_INVALID, "sp_parareal_batch_run: null argument");
     const int n = (int)b->ins.size();
     SP_CUDA(cudaSetDevice(b->device));
