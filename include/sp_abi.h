@@ -262,6 +262,14 @@ int sp_autotune(sp_convection* h, int precision, int batch);
  * and leaves the handle usable.  No counterpart in the reference (which has
  * no bounded waits). */
 int sp_selftest_wait_timeout(sp_convection* h, double limit_ms);
+/* Store-bounds checking, the stand-in for a memory sanitizer: in the library
+ * built with -DSP_BOUNDS_CHECK=1 (libstencilparareal_checked.so) every global
+ * store of the stencil-producing kernels (stage, fused-pair and widening
+ * kernels) is tested against its output allocation and skipped, not made, when
+ * it falls outside.  *checked = 1 in that build, 0 otherwise; *count = such
+ * stores on the current device since the previous call (then reset), after
+ * waiting for the device.  No counterpart in the reference. */
+int sp_store_violations(int* checked, long long* count);
 /* Average duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
  * events around every launch on the handle's stream over `reps` steps (after
  * one untimed step; all steps enqueued before one synchronisation) run on a

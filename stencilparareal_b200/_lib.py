@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libstencilparareal.so")
+# STENCILPARAREAL_LIB selects another build of the library (the bounds-checked
+# libstencilparareal_checked.so next to this file)
+LIB_PATH = os.environ.get("STENCILPARAREAL_LIB") or os.path.join(_HERE, "libstencilparareal.so")
 
 SP_OK = 0
 SP_ERR_INVALID = -1
@@ -100,6 +102,7 @@ _SIGS = {
     "sp_set_tune": (_i, [_vp, _i, _i, _i, _i, _i]),
     "sp_kernel_times": (_i, [_vp, _vp, C.c_double, _i, _i, C.POINTER(C.c_float), C.POINTER(_i)]),
     "sp_selftest_wait_timeout": (_i, [_vp, C.c_double]),
+    "sp_store_violations": (_i, [C.POINTER(_i), C.POINTER(C.c_longlong)]),
     "sp_do_rk4_noalloc": (_i, [C.POINTER(SpParams), _vp, _vp, _d, _d, _i, _vp]),
     "sp_parareal_window_begin": (_i, [_vp, _vp]),
     "sp_parareal_window_fine": (_i, [_vp, _i]),

@@ -15,6 +15,31 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 // Device error word values.
 enum : int { DEV_OK = 0, DEV_WAIT_TIMEOUT = 1 };
 
+// Bounds-checked stores (library built with -DSP_BOUNDS_CHECK=1): every global
+// store of the stencil-producing kernels is tested against the byte range of
+// its output allocation; a store outside it is skipped and counted in this
+// module's violation word (read by sp_store_violations).  Without the flag the
+// test compiles away.
+#ifndef SP_BOUNDS_CHECK
+#define SP_BOUNDS_CHECK 0
+#endif
+struct StoreBounds {
+    const char* lo = nullptr;  // first byte of the output allocation
+    const char* hi = nullptr;  // one past its last byte
+};
+static __device__ unsigned int g_store_violations;
+__device__ __forceinline__ bool store_ok(const StoreBounds& b, const void* p, int bytes) {
+#if SP_BOUNDS_CHECK
+    const char* c = static_cast<const char*>(p);
+    if (c >= b.lo && c + bytes <= b.hi) return true;
+    atomicAdd(&g_store_violations, 1u);
+    return false;
+#else
+    (void)b; (void)p; (void)bytes;
+    return true;
+#endif
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -130,6 +155,17 @@ __device__ __forceinline__ void st16(T* p, const Vec<T, V16<T>::N>& r) {
     } else {
         *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
     }
+}
+
+// Global stores of the stencil-producing kernels, checked against the output
+// allocation `b` when the library is built with SP_BOUNDS_CHECK.
+template <typename T>
+__device__ __forceinline__ void gst1(const StoreBounds& b, T* p, T v) {
+    if (store_ok(b, p, (int)sizeof(T))) *p = v;
+}
+template <typename T>
+__device__ __forceinline__ void gst16(const StoreBounds& b, T* p, const Vec<T, V16<T>::N>& r) {
+    if (store_ok(b, p, 16)) st16<T>(p, r);
 }
 
 // 16-byte shared-memory access by 32-bit shared address (offset OFF bytes).

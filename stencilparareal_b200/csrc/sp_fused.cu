@@ -69,21 +69,23 @@ struct PairArgs {
     double* qout;      // pair 3+4: step result
     long long o_item_stride, o_origin, o_px, o_plane;
     int o_halo;        // image depth written with qout
+    StoreBounds sb_o;  // output allocations (bounds-checked builds): yout or qout,
+    StoreBounds sb_a;  // and aout
     int* err;
 };
 
 // Stores cells (x, x+1) of a row and their x-images within `hd` cells of the
 // x faces; x < ni.
-__device__ __forceinline__ void row_pair(double* row, int ni, int hd, int x, const V2& v) {
-    if (x + 2 <= ni) st16<double>(row + x, v);
-    else row[x] = v.v[0];
+__device__ __forceinline__ void row_pair(const StoreBounds& b, double* row, int ni, int hd, int x, const V2& v) {
+    if (x + 2 <= ni) gst16<double>(b, row + x, v);
+    else gst1(b, row + x, v.v[0]);
     if (x < hd || x + 2 > ni - hd) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int xe = x + e;
             if (xe >= ni) continue;
-            if (xe < hd) row[xe + ni] = v.v[e];
-            if (xe >= ni - hd) row[xe - ni] = v.v[e];
+            if (xe < hd) gst1(b, row + xe + ni, v.v[e]);
+            if (xe >= ni - hd) gst1(b, row + xe - ni, v.v[e]);
         }
     }
 }
@@ -91,8 +93,8 @@ __device__ __forceinline__ void row_pair(double* row, int ni, int hd, int x, con
 // Stores cells (x, x+1) of row (y, z) (x < ni) and their periodic images
 // within `hd` cells of a face (faces, edges and corners): the path of the
 // lanes next to a face; the others store their pair with one 16-byte store.
-__device__ __forceinline__ void store_images_pair(double* base, long long px, long long plane, int ni, int nj,
-                                                  int nk, int hd, int x, int y, int z, const V2& v) {
+__device__ __forceinline__ void store_images_pair(const StoreBounds& b, double* base, long long px, long long plane,
+                                                  int ni, int nj, int nk, int hd, int x, int y, int z, const V2& v) {
     double* row = base + (long long)z * plane + (long long)y * px;
 #pragma unroll
     for (int iz = 0; iz < 3; ++iz) {
@@ -105,7 +107,7 @@ __device__ __forceinline__ void store_images_pair(double* base, long long px, lo
             if (iy == 2 && !(y >= nj - hd)) continue;
             const long long oy = iy == 0 ? 0 : (iy == 1 ? (long long)nj * px : -(long long)nj * px);
             double* r = row + oz + oy;
-            row_pair(r, ni, hd, x, v);
+            row_pair(b, r, ni, hd, x, v);
         }
     }
 }
@@ -398,25 +400,25 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
                 if (live) {
                     const int z = z0 - 4 + v;
                     if (!y_img && z >= hd && z < a.nk - hd) {
-                        st16<double>(ocol, o);
+                        gst16<double>(a.sb_o, ocol, o);
                         if (x_img) {
 #pragma unroll
                             for (int e = 0; e < 2; ++e) {
                                 const int xe = x + e;
-                                if (xe < hd) ocol[e + a.ni] = o.v[e];
-                                if (xe >= a.ni - hd) ocol[e - a.ni] = o.v[e];
+                                if (xe < hd) gst1(a.sb_o, ocol + e + a.ni, o.v[e]);
+                                if (xe >= a.ni - hd) gst1(a.sb_o, ocol + e - a.ni, o.v[e]);
                             }
                         }
                     } else if constexpr (PAIR == 0) {
-                        store_images_pair(a.yout + (long long)b * a.item_stride + a.origin, a.px, a.plane, a.ni,
-                                          a.nj, a.nk, 4, x, y, z, o);
+                        store_images_pair(a.sb_o, a.yout + (long long)b * a.item_stride + a.origin, a.px, a.plane,
+                                          a.ni, a.nj, a.nk, 4, x, y, z, o);
                     } else {
-                        store_images_pair(a.qout + (long long)b * a.o_item_stride + a.o_origin, a.o_px, a.o_plane,
-                                          a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
+                        store_images_pair(a.sb_o, a.qout + (long long)b * a.o_item_stride + a.o_origin, a.o_px,
+                                          a.o_plane, a.ni, a.nj, a.nk, a.o_halo, x, y, z, o);
                     }
                     if constexpr (PAIR == 0) {
-                        if (full) st16<double>(acol, oa);
-                        else acol[0] = oa.v[0];
+                        if (full) gst16<double>(a.sb_a, acol, oa);
+                        else gst1(a.sb_a, acol, oa.v[0]);
                     }
                 }
             }
@@ -460,7 +462,7 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
 // Widening: interior of a caller-layout field -> internal field with every
 // periodic image within 4 cells of a face.
 __global__ void k_widen(double* dst, Geo gd, const double* src, Geo gs, int items, const int* item_lo,
-                        int item_base) {
+                        int item_base, StoreBounds bounds) {
     pdl_trigger();
     pdl_wait();
     const long long n = (long long)gd.ni * gd.nj * gd.nk;
@@ -485,9 +487,9 @@ __global__ void k_widen(double* dst, Geo gd, const double* src, Geo gs, int item
                 if (iy == 2 && !(y >= gd.nj - hd)) continue;
                 const int yy = iy == 0 ? y : (iy == 1 ? y + gd.nj : y - gd.nj);
                 double* r = db + (long long)zz * gd.plane + (long long)yy * gd.px;
-                r[x] = v;
-                if (x < hd) r[x + gd.ni] = v;
-                if (x >= gd.ni - hd) r[x - gd.ni] = v;
+                gst1(bounds, r + x, v);
+                if (x < hd) gst1(bounds, r + x + gd.ni, v);
+                if (x >= gd.ni - hd) gst1(bounds, r + x - gd.ni, v);
             }
         }
     }
@@ -537,11 +539,14 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
         a.c1y = dthalf; a.c2y = dthalf; a.c2a = L.dt / 3.;
         a.yout = static_cast<double*>(L.y2);
         a.aout = static_cast<double*>(L.acc);
+        a.sb_o = out_bounds(a.yout, g4, L.items);
+        a.sb_a = out_bounds(a.aout, g4, L.items);
     } else {          // stages 3 and 4
         a.c1y = L.dt; a.c2a = L.dt / 6.;
         a.qout = static_cast<double*>(L.out);
         a.o_item_stride = go.total; a.o_origin = go.origin; a.o_px = go.px; a.o_plane = go.plane;
         a.o_halo = go.halo;
+        a.sb_o = out_bounds(a.qout, go, L.items);
     }
     a.err = err;
     const long long nct = (total + a.span - 1) / a.span * a.cy;
@@ -564,6 +569,14 @@ unsigned grid_cells(long long n) {
 }  // namespace
 
 bool pair_supported(const Geo& g) { return g.es == 8 && g.ni >= 4 && g.nj >= 4 && g.nk >= 4; }
+
+unsigned long long take_store_violations_pairs() {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_store_violations, sizeof v) != cudaSuccess) return 0;
+    const unsigned int zero = 0;
+    cudaMemcpyToSymbol(g_store_violations, &zero, sizeof zero);
+    return v;
+}
 
 cudaError_t prepare_pairs() {
     cudaError_t e = set_pair_attr<0, 8, 7, 2>();
@@ -593,7 +606,7 @@ cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* sr
     if (g4.es != 8 || gs.es != 8 || items < 1 || items > 65535) return cudaErrorInvalidValue;
     dim3 grid(grid_cells((long long)g4.ni * g4.nj * g4.nk), items);
     return launch_pdl(k_widen, grid, dim3(256), 0, s, static_cast<double*>(dst), g4,
-                      static_cast<const double*>(src), gs, items, item_lo, item_base);
+                      static_cast<const double*>(src), gs, items, item_lo, item_base, out_bounds(dst, g4, items));
 }
 
 }  // namespace sp

@@ -114,6 +114,10 @@ cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const
 cudaError_t launch_widen(const Geo& g4, void* dst, const Geo& gs, const void* src, int items, const int* item_lo,
                          int item_base, cudaStream_t s);
 cudaError_t prepare_pairs();
+// Stores counted outside their output allocation by the bounds-checked build
+// (stage kernels; pair and widening kernels) since the previous call; reset.
+unsigned long long take_store_violations_stages();
+unsigned long long take_store_violations_pairs();
 // One CTA waiting on an mbarrier that never completes, bounded by limit_ns;
 // sets *err to the timeout code (test of the bounded-wait error path).
 cudaError_t launch_wait_selftest(int* err, unsigned long long limit_ns, cudaStream_t s);

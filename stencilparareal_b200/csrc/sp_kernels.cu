@@ -104,6 +104,7 @@ struct KArgs {
     int ni, nj, nk, pz;
     int tiles_x, zchunk, nzc;
     int zrev;         // TMA kernel: CTAs take items and z-chunks in descending order
+    StoreBounds sb_y, sb_a;  // output allocations of yout and aout (bounds-checked builds)
     const int* item_lo;
     int item_base;
     T ca0, ca1, ca2;          // c_d/(12dx)
@@ -199,23 +200,24 @@ __device__ __forceinline__ void cell_op(const KArgs<T>& a, T nl, const Nb<T>& s,
 template <typename T>
 __device__ __forceinline__ void store_images1(T* base, int x, int y, int z, T v, const KArgs<T>& a) {
     T* row = base + (long long)z * a.plane + (long long)y * a.px;
-    row[x] = v;
-    if (x < 2) row[x + a.ni] = v;
-    if (x >= a.ni - 2) row[x - a.ni] = v;
-    if (y < 2) row[(long long)a.nj * a.px + x] = v;
-    if (y >= a.nj - 2) row[-(long long)a.nj * a.px + x] = v;
-    if (z < 2) row[(long long)a.nk * a.plane + x] = v;
-    if (z >= a.nk - 2) row[-(long long)a.nk * a.plane + x] = v;
+    const StoreBounds& b = a.sb_y;
+    gst1(b, row + x, v);
+    if (x < 2) gst1(b, row + x + a.ni, v);
+    if (x >= a.ni - 2) gst1(b, row + x - a.ni, v);
+    if (y < 2) gst1(b, row + (long long)a.nj * a.px + x, v);
+    if (y >= a.nj - 2) gst1(b, row - (long long)a.nj * a.px + x, v);
+    if (z < 2) gst1(b, row + (long long)a.nk * a.plane + x, v);
+    if (z >= a.nk - 2) gst1(b, row - (long long)a.nk * a.plane + x, v);
 }
 
 template <typename T, int N>
-__device__ __forceinline__ void put_vec(T* p, int x, int ni, const Vec<T, N>& v) {
+__device__ __forceinline__ void put_vec(const StoreBounds& b, T* p, int x, int ni, const Vec<T, N>& v) {
     if (x + N <= ni) {
-        st16<T>(p, v);
+        gst16<T>(b, p, v);
     } else {
 #pragma unroll
         for (int e = 0; e < N; ++e)
-            if (x + e < ni) p[e] = v.v[e];
+            if (x + e < ni) gst1(b, p + e, v.v[e]);
     }
 }
 
@@ -224,20 +226,21 @@ template <typename T, int N>
 __device__ __forceinline__ void store_images_vec(T* base, int x, int y, int z, const Vec<T, N>& v, const KArgs<T>& a,
                                                  bool images) {
     T* row = base + (long long)z * a.plane + (long long)y * a.px + x;
-    put_vec<T, N>(row, x, a.ni, v);
+    const StoreBounds& b = a.sb_y;
+    put_vec<T, N>(b, row, x, a.ni, v);
     if (!images) return;
 #pragma unroll
     for (int e = 0; e < N; ++e) {
         const int xe = x + e;
         if (xe < a.ni) {
-            if (xe < 2) row[e + a.ni] = v.v[e];
-            if (xe >= a.ni - 2) row[e - a.ni] = v.v[e];
+            if (xe < 2) gst1(b, row + e + a.ni, v.v[e]);
+            if (xe >= a.ni - 2) gst1(b, row + e - a.ni, v.v[e]);
         }
     }
-    if (y < 2) put_vec<T, N>(row + (long long)a.nj * a.px, x, a.ni, v);
-    if (y >= a.nj - 2) put_vec<T, N>(row - (long long)a.nj * a.px, x, a.ni, v);
-    if (z < 2) put_vec<T, N>(row + (long long)a.nk * a.plane, x, a.ni, v);
-    if (z >= a.nk - 2) put_vec<T, N>(row - (long long)a.nk * a.plane, x, a.ni, v);
+    if (y < 2) put_vec<T, N>(b, row + (long long)a.nj * a.px, x, a.ni, v);
+    if (y >= a.nj - 2) put_vec<T, N>(b, row - (long long)a.nj * a.px, x, a.ni, v);
+    if (z < 2) put_vec<T, N>(b, row + (long long)a.nk * a.plane, x, a.ni, v);
+    if (z >= a.nk - 2) put_vec<T, N>(b, row - (long long)a.nk * a.plane, x, a.ni, v);
 }
 
 template <typename T>
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(32 * TYD) k_stage_direct(const KArgs<T> a) {
             T oy = 0, oa = 0;
             cell_op<T, OP>(a, nl, s, p0, p1, p2, oy, oa, g, true);
             store_images1<T>(a.yout + ob, x, y, z, oy, a);
-            if constexpr (OpTraits<OP>::writes_a) a.aout[off] = oa;
+            if constexpr (OpTraits<OP>::writes_a) gst1(a.sb_a, a.aout + off, oa);
             zm2 = zm1; zm1 = zc0; zc0 = zp1; zp1 = zp2;
         }
     }
@@ -519,20 +522,20 @@ __global__ void __launch_bounds__(32 * TY)
         }
         if (live) {
             if (!y_img && z >= 2 && z < a.nk - 2) {
-                st16<T>(yrow_out, oy);
+                gst16<T>(a.sb_y, yrow_out, oy);
                 if (x_img) {
 #pragma unroll
                     for (int e = 0; e < VX; ++e) {
-                        if (x + e < 2) yrow_out[e + a.ni] = oy.v[e];
-                        if (x + e >= a.ni - 2) yrow_out[e - a.ni] = oy.v[e];
+                        if (x + e < 2) gst1(a.sb_y, yrow_out + e + a.ni, oy.v[e]);
+                        if (x + e >= a.ni - 2) gst1(a.sb_y, yrow_out + e - a.ni, oy.v[e]);
                     }
                 }
             } else {
                 store_images_vec<T, VX>(a.yout + ob, x, y, z, oy, a, true);
             }
             if constexpr (OpTraits<OP>::writes_a) {
-                if (full_vec) st16<T>(arow_out, oa);
-                else put_vec<T, VX>(arow_out, x, a.ni, oa);
+                if (full_vec) gst16<T>(a.sb_a, arow_out, oa);
+                else put_vec<T, VX>(a.sb_a, arow_out, x, a.ni, oa);
             }
         }
         yrow_out += a.plane;
@@ -618,6 +621,7 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err)
     // RK4 stages alternate the sweep direction (S1, S3 descending; S2, S4 ascending),
     // so that each stage starts on the planes the previous one touched last
     a.zrev = (L.op == OP_RK_S1 || L.op == OP_RK_S3) ? 1 : 0;
+    a.sb_y = out_bounds(L.yout, g, L.items);
     fill_w13<T>(a.w, c, L.nu);  // RHS4 as per-offset weights (TMA RK stages; one nu per launch)
     switch (L.op) {
         case OP_RK_S1: break;
@@ -633,6 +637,7 @@ KArgs<T> make_args(const Geo& g, const StageLaunch& L, const Shape& t, int* err)
         case OP_ADJ + 3: a.pw0 = (const T*)L.ypt; a.pw1 = (const T*)L.lam_acc; break;
         default: break;
     }
+    a.sb_a = out_bounds(a.aout, g, L.items);
     if (L.op >= OP_ADJ) {
         a.c_y = (T)L.c_ybar;
         a.c_acc = (T)L.c_lam;
@@ -740,6 +745,14 @@ cudaError_t launch_T(const Geo& g, const StageLaunch& L, const Shape& t, cudaStr
 }
 
 }  // namespace
+
+unsigned long long take_store_violations_stages() {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_store_violations, sizeof v) != cudaSuccess) return 0;
+    const unsigned int zero = 0;
+    cudaMemcpyToSymbol(g_store_violations, &zero, sizeof zero);
+    return v;
+}
 
 cudaError_t prepare_kernels() {
     cudaError_t e = cudaSuccess;

@@ -662,6 +662,18 @@ int sp_field_errors(sp_convection* h, const double* a, const double* b, double* 
 // Error-path self-test: a kernel whose wait can never complete gives up after
 // limit_ms; the call returns the status the handle then reports (SP_ERR_TIMEOUT)
 // and leaves the handle usable.
+extern "C" int sp_store_violations(int* checked, long long* count) {
+    if (!checked || !count) return fail(SP_ERR_INVALID, "null argument");
+#if defined(SP_BOUNDS_CHECK) && SP_BOUNDS_CHECK
+    *checked = 1;
+#else
+    *checked = 0;
+#endif
+    SP_CUDA(cudaDeviceSynchronize());
+    *count = (long long)(take_store_violations_stages() + take_store_violations_pairs());
+    return SP_OK;
+}
+
 extern "C" int sp_selftest_wait_timeout(sp_convection* h, double limit_ms) {
     int rc = check_handle(h);
     if (rc) return rc;

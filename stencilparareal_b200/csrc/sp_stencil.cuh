@@ -6,6 +6,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <utility>
 
 #include "sp_device.cuh"
@@ -72,6 +73,27 @@ cudaError_t launch_pdl(void (*k)(KP...), dim3 grid, dim3 block, size_t smem, cud
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
+// Byte range of `items` fields of geometry g from `base`: the allocation a
+// launch writes, checked by the bounds-checked build's stores.  In that build
+// SP_BOUNDS_SHRINK_PLANES=n (environment) narrows the range by n planes at its
+// top, so that a test can see the checker count (and skip) stores that lie
+// inside the real allocation.
+inline StoreBounds out_bounds(const void* base, const Geo& g, int items) {
+    StoreBounds b;
+    if (!base) return b;
+    b.lo = static_cast<const char*>(base);
+    long long bytes = (long long)items * g.total * g.es;
+#if SP_BOUNDS_CHECK
+    static const long long shrink = [] {
+        const char* e = std::getenv("SP_BOUNDS_SHRINK_PLANES");
+        return e ? std::atoll(e) : 0LL;
+    }();
+    bytes -= shrink * g.plane * g.es;
+#endif
+    b.hi = b.lo + bytes;
+    return b;
 }
 
 // Tensor map over `items` fields of geometry g starting at `base`: dims
