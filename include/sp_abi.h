@@ -252,9 +252,9 @@ long long sp_launch_count(void);
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* kind);
 /* Runs the autotuner for this handle's grid at `batch` fields and precision: every
  * stage kernel gets the fastest of its candidate launch shapes, and FP64 RK4
- * steps run as fused pairs when those are faster than the four stages: for
- * batch 1 as timed through sp_do_rk4 (a graph chunk of 50 steps on scratch
- * fields), for larger batches over four consecutive batched steps. */
+ * steps run as fused pairs when those are more than 2 % faster than the four
+ * stages: for batch 1 as timed through sp_do_rk4 (a graph chunk of 50 steps on
+ * scratch fields), for larger batches over four consecutive batched steps. */
 int sp_autotune(sp_convection* h, int precision, int batch);
 /* Test of the error path of the bounded in-kernel waits: runs one kernel whose
  * wait can never complete and gives up after limit_ms (<= 2000); returns
