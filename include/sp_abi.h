@@ -270,7 +270,7 @@ int sp_selftest_wait_timeout(sp_convection* h, double limit_ms);
  * stores on the current device since the previous call (then reset), after
  * waiting for the device.  No counterpart in the reference. */
 int sp_store_violations(int* checked, long long* count);
-/* Average duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
+/* Median duration in ms of each kernel of an FP64 RK4 step, timed with CUDA
  * events around every launch on the handle's stream over `reps` steps (after
  * one untimed step; all steps enqueued before one synchronisation) run on a
  * copy of `field` (which is left unchanged).  path 0: the kernels the handle's

@@ -701,7 +701,7 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
     const Geo& g = h->g[0];
     const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
     int* err = h->err.as<int>();
-    float acc[4] = {0, 0, 0, 0};
+    std::vector<float> times[4];  // per kernel, one duration per timed rep
     if (path == 2 && !pair_supported(h->g4)) return fail(SP_ERR_INVALID, "fused pairs need >= 4 cells per axis");
     const bool fused = path == 2 || (path == 0 && t.fused && pair_supported(h->g4));
     if (fused) {
@@ -762,13 +762,20 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
         for (int k = 0; k < nk; ++k) {
             float m = 0;
             cudaEventElapsedTime(&m, ev[(size_t)r * nk + k], ev[(size_t)r * nk + k + 1]);
-            acc[k] += m;
+            times[k].push_back(m);
         }
     *count = nk;
     for (auto& x : ev)
         if (x) cudaEventDestroy(x);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, "kernel timing: %s", cudaGetErrorString(e));
-    for (int k = 0; k < *count; ++k) ms[k] = acc[k] / reps;
+    // the median: a rep in which the host fell behind the GPU (the GPU idling
+    // inside an event interval) does not move it
+    for (int k = 0; k < *count; ++k) {
+        std::vector<float>& v = times[k];
+        std::sort(v.begin(), v.end());
+        const size_t h = v.size() / 2;
+        ms[k] = v.empty() ? 0.f : (v.size() % 2 ? v[h] : 0.5f * (v[h - 1] + v[h]));
+    }
     return sp_convection_synchronize(h);
 }
 
