@@ -440,7 +440,7 @@ def main():
 
     peak, peak_kind = peaks()
     # roofline of the dominant kernel: its algorithmic bytes per launch over its
-    # average launch time, every kernel of a step timed with CUDA events on the
+    # median launch time, every kernel of a step timed with CUDA events on the
     # library's stream
     ktimes = conv.kernel_times(fin, DT, reps=20)
     dom = max(ktimes, key=ktimes.get)
