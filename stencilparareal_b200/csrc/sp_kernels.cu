@@ -318,12 +318,13 @@ __global__ void __launch_bounds__(32 * TYD) k_stage_direct(const KArgs<T> a) {
 
 // ---------------------------------------------------------------------------
 // TMA stage kernel.  Block = 32*TY threads (warp w owns tile row w), grid
-// (tiles_x*tiles_y, nzc, items).  Shared memory: NS stencil-input slots of
-// (TX+2LX) x (TY+4) elements and NP pointwise slots of npw x TX x TY elements,
-// followed by NS+NP mbarriers.  Ring bookkeeping uses running slot indices
-// and phase bits instead of divisions; CTAs whose tile is two or more cells
-// away from every x/y face skip the periodic-image logic except on the four
-// planes next to the z faces.
+// (tiles_x*tiles_y, nzc, items), taken in descending item / z-chunk order when
+// zrev is set.  Shared memory: NS stencil-input slots of (TX+2LX) x (TY+4)
+// elements and NP pointwise slots of npw x TX x TY elements, followed by NS+NP
+// mbarriers.  Ring bookkeeping uses running slot indices and phase bits instead
+// of divisions; lanes whose cells are two or more cells away from every y face
+// store one 16-byte vector (plus the x images of cells next to an x face)
+// except on the four planes next to the z faces.
 
 
 template <typename T, int OP, int TY, int NS, int NP>
