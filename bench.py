@@ -137,15 +137,18 @@ def run_reference(args, rank, world):
     n = N_FINE
     steps = 8  # bounded sample per step: 8 RK4 steps of the 256^3 workload (a few s on the host cores)
     p = O.params(n, dx=1.0 / n, nu0=NU, nufreq=0.0, cx=C[0], cy=C[1], cz=C[2])
-    q = fourier_ic(n)
+    # the propagator and its fields are allocated and loaded once, outside the
+    # timed region, as the reference's drivers construct Convection and the
+    # fields before they time DoRK4 (src/Parareal/main.cpp:187-189,218-222)
+    sess = O.RK4Session(p, fourier_ic(n))
     for _ in range(args.warmup):
-        q1 = O.rk4(p, q, 0.0, DT, steps)
+        sess.run(0.0, DT, steps)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        q1 = O.rk4(p, q, 0.0, DT, steps)
+        sess.run(0.0, DT, steps)
         times.append(time.perf_counter() - t0)
-    del q1
+    sess.close()
     tot = sum(times)
     val = n ** 3 * steps * args.steps / tot / 1e9
     line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -153,7 +156,8 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "sample": f"{steps} RK4 steps of {n}^3 per step"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
-                             "sample": f"{steps} RK4 steps of {n}^3 per timed step, {args.steps} steps"},
+                             "sample": f"{steps} RK4 steps of {n}^3 per timed step on fields allocated once, "
+                                       f"{args.steps} steps"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -166,12 +170,15 @@ def cpu_baseline_sample():
     O.set_threads(cores)
     n, steps = N_FINE, 24
     p = O.params(n, dx=1.0 / n, nu0=NU, nufreq=0.0, cx=C[0], cy=C[1], cz=C[2])
-    q = fourier_ic(n)
+    sess = O.RK4Session(p, fourier_ic(n))
+    sess.run(0.0, DT, 1)  # untimed: first sweep over freshly mapped pages
     t0 = time.perf_counter()
-    O.rk4(p, q, 0.0, DT, steps)
+    sess.run(0.0, DT, steps)
     dt = time.perf_counter() - t0
+    sess.close()
     return {"value": n ** 3 * steps / dt / 1e9, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
-            "sample": f"{steps} RK4 steps of {n}^3 (oracle restating the reference OpenMP path), {dt:.1f} s"}
+            "sample": f"{steps} RK4 steps of {n}^3 on fields allocated once (oracle restating the reference "
+                      f"OpenMP path), {dt:.1f} s"}
 
 
 def cpu_vs_gpu_times(torch, sp, device, gpu_serial_128_s=None):
@@ -214,7 +221,13 @@ def cpu_vs_gpu_times(torch, sp, device, gpu_serial_128_s=None):
 
 
 def parareal_summary(torch, sp, device):
-    """Parareal on one GPU: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice)."""
+    """Parareal on one GPU: 128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (rounded to 7 steps/slice).
+
+    Two stopping rules: "reference" stops once the last slice is within 1e-8
+    relative L2 of the serial FP64 fine solution (the configuration's own
+    criterion; a real run does not have that solution), "defect" stops once
+    every slice end changed by less than 1e-8 relative L2 in the last
+    iteration (what a user without the serial solution can run)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     n, P, T = 128, 32, 0.2
@@ -226,37 +239,45 @@ def parareal_summary(torch, sp, device):
                                    timeStepsCoarse=200, kmax=8)
     q0, qs, q = conv.field(), conv.field(), conv.field()
     conv.upload(q0, gaussian_noise(n, seed=0))
-    par = sp.Parareal(conv, q0, q, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
-                      tol_kind="reference", skip_converged=True)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    par.DoSerial()  # warm (graphs)
+    par = {rule: sp.Parareal(conv, q0, q, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
+                             tol_kind=rule, skip_converged=True) for rule in ("reference", "defect")}
+    ser = sp.Parareal(conv, q0, qs, 0.0, conf)
+    ser.DoSerial()  # warm (graphs)
     conv.synchronize()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    par.DoSerial()
+    ser.DoSerial()
     conv.synchronize()
     t_serial = time.perf_counter() - t0
-    ref = par.solution
-    qs.data.copy_(ref.data)
-    par.solution = q
-    rep = par.DoParallel(reference=qs)  # warm (graph capture)
-    rep = par.DoParallel(reference=qs)
-    del ev
-    return {"config": "128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5 (625 steps/slice), coarse RK4 FP32 "
-                      "dt=0.2/224 (200 rounded up to 224 total, 7 steps/slice), Gaussian+noise IC seed 0, "
-                      "c=(1,1,1), nu=0.01",
-            "serial_fine_s": t_serial, "parareal_s": rep["seconds"], "iterations": rep["iterations"],
-            "err_l2_vs_serial": rep["err_l2"][-1] if rep["err_l2"] else None,
-            "defects": rep["defect"], "err_l2": rep["err_l2"],
-            "speedup_vs_serial": t_serial / rep["seconds"] if rep["seconds"] else None,
-            "fine_s": rep["seconds_fine"], "coarse_s": rep["seconds_coarse"]}
+    out = {"config": "128^3, P=32, T=0.2, fine RK4 FP64 dt=1e-5 (625 steps/slice), coarse RK4 FP32 "
+                     "dt=0.2/224 (200 rounded up to 224 total, 7 steps/slice), increment-form correction, "
+                     "Gaussian+noise IC seed 0, c=(1,1,1), nu=0.01",
+           "serial_fine_s": t_serial}
+    for rule, pr in par.items():
+        pr.DoParallel(reference=qs)  # warm (graph capture)
+        rep = pr.DoParallel(reference=qs)
+        r = {"parareal_s": rep["seconds"], "iterations": rep["iterations"],
+             "err_l2_vs_serial": rep["err_l2"][-1] if rep["err_l2"] else None,
+             "defects": rep["defect"], "err_l2": rep["err_l2"],
+             "speedup_vs_serial": t_serial / rep["seconds"] if rep["seconds"] else None,
+             "fine_s": rep["seconds_fine"], "coarse_s": rep["seconds_coarse"],
+             "fine_gcups": rep["fine_cell_updates"] / rep["seconds_fine"] / 1e9 if rep["seconds_fine"] else None}
+        if rule == "reference":
+            out.update(r)  # the configuration's own criterion: the headline fields
+            out["stop_rule"] = "reference: last slice within 1e-8 rel. L2 of the serial FP64 fine solution"
+        else:
+            r["stop_rule"] = "defect: every slice end changed by < 1e-8 rel. L2 in the last iteration"
+            out["defect_rule"] = r
+    out["serial_fine_gcups"] = n ** 3 * 20000 / t_serial / 1e9
+    return out
 
 
 def batch_summary(torch, sp, device, n_inst=48, seed=2):
     """Batched uneven instances: 48 independent Parareal solves, grids drawn from {32,48,64,96}^3, nu log-uniform in
     [1e-4, 1e-2], c uniform in [-1,1]^3, 8-24 slices; T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32
     dt=1e-3 (totals rounded up to a multiple of the slice count), tolerance 1e-8 relative L2 against
-    each instance's serial FP64 fine solution."""
+    each instance's serial FP64 fine solution ("reference" rule), and the same batch stopped by the
+    1e-8 defect rule."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     from stencilparareal_b200.parareal import PararealBatch
@@ -270,7 +291,8 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
         P = int(rng.integers(8, 25))
         specs.append((n, nu, tuple(float(v) for v in c), P))
     tunes = {}
-    inst, refs, serial_s = [], [], 0.0
+    inst = {"reference": [], "defect": []}
+    refs, serial_s = [], 0.0
     for i, (n, nu, c, P) in enumerate(specs):
         conv = sp.Convection(n, n, n, 1.0 / n, nu, 0.0, *c, device=device)
         if n not in tunes:
@@ -282,32 +304,41 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
         conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
         conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu, gridSize=n, endTime=T, timeStepsFine=5000,
                                        timeStepsCoarse=50, kmax=P)
-        f0, fs, fr = conv.field(), conv.field(), conv.field()
+        f0, fs, fr, fd = conv.field(), conv.field(), conv.field(), conv.field()
         conv.upload(f0, gaussian_noise(n, seed=seed + i))
-        par = sp.Parareal(conv, f0, fs, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
-                          tol_kind="reference")
+        ser = sp.Parareal(conv, f0, fr, 0.0, conf)
         t0 = time.perf_counter()
-        par.DoSerial()
+        ser.DoSerial()
         conv.synchronize()
         serial_s += time.perf_counter() - t0
-        fr.data.copy_(fs.data)
-        inst.append(par)
+        for rule, sol in (("reference", fs), ("defect", fd)):
+            inst[rule].append(sp.Parareal(conv, f0, sol, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8,
+                                          tol_kind=rule))
         refs.append(fr)
-    batch = PararealBatch(inst)
-    reps, secs = batch.run(references=refs)   # warm (first launch)
-    reps, secs = batch.run(references=refs)
-    fine_cu = sum(r["fine_cell_updates"] for r in reps)
-    its = [r["iterations"] for r in reps]
-    errs = [r["err_l2"][-1] for r in reps]
-    return {"config": f"{n_inst} instances, grids {{32,48,64,96}}^3, nu log-uniform [1e-4,1e-2], c U[-1,1]^3, "
-                      "P 8-24, T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 dt=1e-3 (rounded per P), "
-                      "increment-form correction, stop at 1e-8 rel L2 vs serial fine; seed 2",
-            "instances": n_inst, "batch_s": secs, "serial_fine_sum_s": serial_s,
-            "speedup_vs_serial_sum": serial_s / secs if secs else None,
-            "iterations_max": max(its), "iterations_mean": sum(its) / len(its),
-            "err_l2_max": max(errs), "fine_gcups": fine_cu / secs / 1e9,
-            "grids": {str(k): sum(1 for s_ in specs if s_[0] == k) for k in (32, 48, 64, 96)},
-            "tunes": {str(k): v[0] for k, v in tunes.items()}}
+    out = {"config": f"{n_inst} instances, grids {{32,48,64,96}}^3, nu log-uniform [1e-4,1e-2], c U[-1,1]^3, "
+                     "P 8-24, T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 dt=1e-3 (rounded per P), "
+                     "increment-form correction, stop at 1e-8 rel L2 vs serial fine; seed 2",
+           "instances": n_inst, "serial_fine_sum_s": serial_s,
+           "grids": {str(k): sum(1 for s_ in specs if s_[0] == k) for k in (32, 48, 64, 96)},
+           "tunes": {str(k): v[0] for k, v in tunes.items()}}
+    for rule in ("reference", "defect"):
+        batch = PararealBatch(inst[rule])
+        batch.run(references=refs)   # warm (first launch)
+        reps, secs = batch.run(references=refs)
+        fine_cu = sum(r["fine_cell_updates"] for r in reps)
+        its = [r["iterations"] for r in reps]
+        errs = [r["err_l2"][-1] for r in reps]
+        r = {"batch_s": secs, "speedup_vs_serial_sum": serial_s / secs if secs else None,
+             "iterations_max": max(its), "iterations_mean": sum(its) / len(its),
+             "err_l2_max": max(errs), "fine_gcups": fine_cu / secs / 1e9}
+        if rule == "reference":
+            out.update(r)
+            out["stop_rule"] = "reference: within 1e-8 rel. L2 of each instance's serial FP64 fine solution"
+        else:
+            r["stop_rule"] = "defect: every slice end changed by < 1e-8 rel. L2 in the last iteration"
+            out["defect_rule"] = r
+        del batch
+    return out
 
 
 def adjoint_summary(torch, sp, device):

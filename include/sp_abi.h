@@ -230,11 +230,15 @@ int sp_adjoint_rk4(sp_convection* h, const double* q0, const double* q_target, c
  * process exits.  Grids whose three FP64 work fields do not fit (beyond about
  * 80^3) are rejected with SP_ERR_INVALID.  `in`/`out` are FP64 fields in the
  * sp_field_layout geometry on the current device; the call runs on `stream`
- * (NULL = legacy default stream) and returns when the steps are done.  The
- * first call on each device looks up the array's device address and sets the
- * kernels' shared-memory limits; make that first call before any stream
- * capture.  All calls share the one array: calls whose GPU work overlaps
- * (other streams, other host threads) race on it. */
+ * (NULL = legacy default stream) and returns when the steps are done: each
+ * call synchronizes `stream` to read back the error word of its bounded
+ * in-kernel waits (SP_ERR_TIMEOUT).  The first call on each device looks up
+ * the array's device address and sets the kernels' shared-memory limits; make
+ * that first call before any stream capture.  A first call that fails leaves
+ * nothing behind: the next call on that device sets up again.  GPUs older
+ * than sm_100 are rejected with SP_ERR_UNSUPPORTED, as by
+ * sp_convection_create.  All calls share the one array: calls whose GPU work
+ * overlaps (other streams, other host threads) race on it. */
 #define SP_NOALLOC_SCRATCH_BYTES (16u << 20)
 int sp_do_rk4_noalloc(const sp_params* p, const double* in, double* out, double tStart, double dt, int timesteps,
                       void* stream);

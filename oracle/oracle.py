@@ -73,6 +73,16 @@ def lib():
         L.orc_parareal_derived.restype = i
         L.orc_parareal.argtypes = [P(OrcParams), P(OrcPararealCfg), dp, dp, dp, dp, dp]
         L.orc_parareal.restype = i
+        L.orc_parareal_ex.argtypes = [P(OrcParams), P(OrcPararealCfg), dp, dp, dp, dp, dp, dp, dp]
+        L.orc_parareal_ex.restype = i
+        L.orc_rk4_session_create.argtypes = [P(OrcParams), dp]
+        L.orc_rk4_session_create.restype = C.c_void_p
+        L.orc_rk4_session_run.argtypes = [C.c_void_p, d, d, i]
+        L.orc_rk4_session_run.restype = i
+        L.orc_rk4_session_result.argtypes = [C.c_void_p, dp]
+        L.orc_rk4_session_result.restype = i
+        L.orc_rk4_session_destroy.argtypes = [C.c_void_p]
+        L.orc_rk4_session_destroy.restype = None
         L.orc_adjoint_rk4.argtypes = [P(OrcParams), dp, dp, d, d, i, dp, dp, dp]
         L.orc_adjoint_rk4.restype = i
         L.orc_exactq.argtypes = [d] * 9
@@ -191,6 +201,56 @@ def parareal(p, cfg, q0):
     _check(lib().orc_parareal(C.byref(p), C.byref(cfg), _ptr(q0), _ptr(q), _ptr(qs), _ptr(em), _ptr(el)),
            "parareal")
     return q, qs, em[:cfg.kmax], el[:cfg.kmax]
+
+
+def parareal_iters(p, cfg, q0):
+    """orc_parareal_ex: Parareal with the per-iteration defect and last-slice fields.
+
+    Returns (q_serial, err_max[kmax], err_l2[kmax], defect[kmax], q_iters[kmax, nk, nj, ni])."""
+    q0 = np.ascontiguousarray(q0, dtype=np.float64)
+    k = max(cfg.kmax, 1)
+    q = np.empty_like(q0)
+    qs = np.empty_like(q0)
+    em, el, de = np.zeros(k), np.zeros(k), np.zeros(k)
+    qi = np.empty((k,) + q0.shape)
+    _check(lib().orc_parareal_ex(C.byref(p), C.byref(cfg), _ptr(q0), _ptr(q), _ptr(qs), _ptr(em), _ptr(el),
+                                 _ptr(de), _ptr(qi)), "parareal_ex")
+    n = cfg.kmax
+    return qs, em[:n], el[:n], de[:n], qi[:n]
+
+
+class RK4Session:
+    """A propagator whose fields are allocated and loaded once (orc_rk4_session):
+    run() performs DoRK4(in, out, t0, dt, n) on the held fields, timing only the
+    steps, as the reference's drivers time DoRK4 on fields they allocated
+    up front (src/Parareal/main.cpp:187-189,218-222)."""
+
+    def __init__(self, p, q):
+        self._p = p
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.shape == _shape(p), (q.shape, _shape(p))
+        self._h = lib().orc_rk4_session_create(C.byref(p), _ptr(q))
+        if not self._h:
+            raise ValueError("oracle session create failed")
+
+    def run(self, t0, dt, n):
+        _check(lib().orc_rk4_session_run(self._h, t0, dt, int(n)), "session run")
+
+    def result(self):
+        out = np.empty(_shape(self._p))
+        _check(lib().orc_rk4_session_result(self._h, _ptr(out)), "session result")
+        return out
+
+    def close(self):
+        if self._h:
+            lib().orc_rk4_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def adjoint_rk4(p, q0, q_target, t0, dt, n):

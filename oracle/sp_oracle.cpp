@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <utility>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -28,18 +29,39 @@ constexpr int kHalo = 2;
 
 // Halo-padded field in the reference's OpenMP storage order JIK: j slowest,
 // i middle, k fastest (SharedInfrastructure.h:76-80, Convection.h:19).
+// Allocator whose value-initialisation is a no-op, so that a field's pages are
+// first touched by the parallel zero-fill in Field::init (the threads that
+// later sweep the same j-rows), not by one thread in std::vector's constructor.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) {}
+    template <typename U>
+    void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+
 template <typename T>
 struct Field {
     int ni = 0, nj = 0, nk = 0;
     long si = 0, sj = 0;  // strides of i and j; k stride is 1
-    std::vector<T> v;
+    std::vector<T, NoInitAlloc<T>> v;
     Field() = default;
     Field(int a, int b, int c) { init(a, b, c); }
     void init(int a, int b, int c) {
         ni = a; nj = b; nk = c;
         si = nk + 2 * kHalo;
         sj = (long)(ni + 2 * kHalo) * si;
-        v.assign((size_t)(nj + 2 * kHalo) * sj, T(0));
+        const long rows = nj + 2 * kHalo;
+        v.resize((size_t)rows * sj);
+        T* d = v.data();
+        const long row = sj;
+#pragma omp parallel for schedule(static)
+        for (long j = 0; j < rows; ++j) std::fill(d + j * row, d + (j + 1) * row, T(0));
     }
     // (i,j,k) are interior coordinates; -2..n+1 address the halo.
     inline T* col(int i, int j) { return v.data() + (long)(j + kHalo) * sj + (long)(i + kHalo) * si + kHalo; }
@@ -507,6 +529,33 @@ int orc_periodicity_jik(int ni, int nj, int nk, double* field) {
     return 0;
 }
 
+struct orc_rk4_session {
+    Convection<double> c;
+    Field<double> fin, fout;
+    explicit orc_rk4_session(const orc_params& p) : c(p), fin(p.ni, p.nj, p.nk), fout(p.ni, p.nj, p.nk) {}
+};
+
+orc_rk4_session* orc_rk4_session_create(const orc_params* p, const double* in) {
+    if (!valid(p) || !in) return nullptr;
+    orc_rk4_session* s = new orc_rk4_session(*p);
+    load_dense(s->fin, in);
+    return s;
+}
+
+int orc_rk4_session_run(orc_rk4_session* s, double tStart, double dt, int n) {
+    if (!s || n < 0) return -1;
+    s->c.DoRK4(s->fin, s->fout, tStart, dt, n);
+    return 0;
+}
+
+int orc_rk4_session_result(const orc_rk4_session* s, double* out) {
+    if (!s || !out) return -1;
+    store_dense(s->fout, out);
+    return 0;
+}
+
+void orc_rk4_session_destroy(orc_rk4_session* s) { delete s; }
+
 int orc_parareal_derived(const orc_parareal_cfg* c, int out[4], double dout[3]) {
     Derived d;
     if (!derive(c, &d)) return -1;
@@ -517,6 +566,11 @@ int orc_parareal_derived(const orc_parareal_cfg* c, int out[4], double dout[3]) 
 
 int orc_parareal(const orc_params* p, const orc_parareal_cfg* c, const double* q0, double* q_out,
                  double* q_serial, double* err_max, double* err_l2) {
+    return orc_parareal_ex(p, c, q0, q_out, q_serial, err_max, err_l2, nullptr, nullptr);
+}
+
+int orc_parareal_ex(const orc_params* p, const orc_parareal_cfg* c, const double* q0, double* q_out,
+                    double* q_serial, double* err_max, double* err_l2, double* defect, double* q_iters) {
     Derived d;
     if (!valid(p) || !derive(c, &d) || !q0 || !q_out) return -1;
     if (c->coarse < 0 || c->coarse > 3) return -1;
@@ -551,6 +605,44 @@ int orc_parareal(const orc_params* p, const orc_parareal_cfg* c, const double* q
         coarse.prop64(U[r], U[r], 0., d.dtC, d.tsC * r);
         coarse.prop64(U[r], Gold[r], tStart, d.dtC, d.tsC);
     }
+    // Slice-end values before iteration 1 (for the defect of iteration 1): the
+    // predictor's U_{r+1}, and G(U_{P-1}) at the last slice's end.
+    std::vector<Field<double>> Qprev;
+    if (defect) {
+        Qprev.resize(P);
+        for (int r = 0; r < P; ++r) Qprev[r].v = (r + 1 < P ? U[r + 1].v : Gold[P - 1].v);
+        for (int r = 0; r < P; ++r) {
+            Qprev[r].ni = p->ni; Qprev[r].nj = p->nj; Qprev[r].nk = p->nk;
+            Qprev[r].si = U[0].si; Qprev[r].sj = U[0].sj;
+        }
+    }
+    // Per iteration: the defect max_r ||Q_r^k - Q_r^{k-1}||_2 / ||Q_r^k||_2 over
+    // the slice ends, and the last slice's result as a dense field.
+    const long ncell = (long)p->ni * p->nj * p->nk;
+    auto record = [&](int k) {
+        if (err_max) err_max[k] = err_maxrel_field(Q[P - 1], qref);
+        if (err_l2) err_l2[k] = err_l2rel_field(Q[P - 1], qref);
+        if (q_iters) store_dense(Q[P - 1], q_iters + (size_t)k * ncell);
+        if (defect) {
+            double dm = 0.;
+            for (int r = 0; r < P; ++r) {
+                double num = 0., den = 0.;
+                for (int j = 0; j < p->nj; ++j)
+                    for (int i = 0; i < p->ni; ++i) {
+                        const double* a = Q[r].col(i, j);
+                        const double* b = Qprev[r].col(i, j);
+                        for (int kk = 0; kk < p->nk; ++kk) {
+                            const double e = a[kk] - b[kk];
+                            num += e * e;
+                            den += a[kk] * a[kk];
+                        }
+                    }
+                if (den > 0) dm = std::max(dm, std::sqrt(num / den));
+                Qprev[r].v = Q[r].v;
+            }
+            defect[k] = dm;
+        }
+    };
     // Increment form of the correction: U_{r+1} = F(U_r^old) + G(U_r^new - U_r^old).
     // G is linear (linear PDE), so this equals the reference's
     // G(U_r^new) + F(U_r^old) - G(U_r^old) in exact arithmetic.
@@ -575,8 +667,7 @@ int orc_parareal(const orc_params* p, const orc_parareal_cfg* c, const double* q
                 coarse.prop64(delta, gd, tStart, d.dtC, d.tsC);
                 for (size_t i = 0; i < gd.v.size(); ++i) Q[r].v[i] = Fq[r].v[i] + gd.v[i];
             }
-            if (err_max) err_max[k] = err_maxrel_field(Q[P - 1], qref);
-            if (err_l2) err_l2[k] = err_l2rel_field(Q[P - 1], qref);
+            record(k);
         }
         store_dense(Q[P - 1], q_out);
         return 0;
@@ -611,8 +702,7 @@ int orc_parareal(const orc_params* p, const orc_parareal_cfg* c, const double* q
             }
             std::swap(Gold[r].v, Gnew[r].v);  // qcoarseold.SwapWith(qcoarsenew)
         }
-        if (err_max) err_max[k] = err_maxrel_field(Q[P - 1], qref);
-        if (err_l2) err_l2[k] = err_l2rel_field(Q[P - 1], qref);
+        record(k);
     }
     store_dense(Q[P - 1], q_out);
     return 0;

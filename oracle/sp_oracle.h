@@ -90,6 +90,26 @@ int orc_parareal_derived(const orc_parareal_cfg* c, int out[4], double dout[3]);
 int orc_parareal(const orc_params* p, const orc_parareal_cfg* c, const double* q0,
                  double* q_out, double* q_serial, double* err_max, double* err_l2);
 
+/* orc_parareal with two more outputs (each may be NULL): defect[k] = max over
+ * slices r of ||Q_r^{k+1} - Q_r^k||_2 / ||Q_r^{k+1}||_2, the relative change of
+ * every slice's end value in iteration k+1 (Q_r^0: the predictor's slice-end
+ * values), and q_iters[k*N .. (k+1)*N) = the last slice's result after
+ * iteration k+1 as a dense array (N = ni*nj*nk). */
+int orc_parareal_ex(const orc_params* p, const orc_parareal_cfg* c, const double* q0,
+                    double* q_out, double* q_serial, double* err_max, double* err_l2,
+                    double* defect, double* q_iters);
+
+/* A propagator with its fields allocated once, as the reference's drivers hold
+ * a Convection object and its fields across calls (Convection.cpp:131-143,
+ * src/Parareal/main.cpp:187-189, timed steps only at main.cpp:218-222):
+ * create loads `in`; every run performs DoRK4(in, out, tStart, dt, n) on the
+ * held fields; result copies `out` into a dense array. */
+typedef struct orc_rk4_session orc_rk4_session;
+orc_rk4_session* orc_rk4_session_create(const orc_params* p, const double* in);
+int orc_rk4_session_run(orc_rk4_session* s, double tStart, double dt, int n);
+int orc_rk4_session_result(const orc_rk4_session* s, double* out);
+void orc_rk4_session_destroy(orc_rk4_session* s);
+
 /* Discrete adjoint of n FP64 RK4 steps (Convection.cpp:318-370) for
  * J = 0.5*||q_n - q_target||^2.  Returns J in *J; grad_q0 gets dJ/dq0 and
  * grad_par[0..3] = dJ/d(nu0, cx, cy, cz).  Stores every step (small grids only). */

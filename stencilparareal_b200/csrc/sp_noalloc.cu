@@ -17,7 +17,10 @@
 // example on two streams, or from two host threads) race on it and corrupt
 // each other's results.  Each call overwrites every scratch cell it later
 // reads, so the contents left by the previous call do not matter; only the
-// error word is cleared at the start of each call.
+// error word is cleared at the start of each call.  Every call waits for
+// its stream before it returns: it reads the error word of the bounded
+// in-kernel waits back to the host, as sp_convection_synchronize does for a
+// handle.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -40,32 +43,39 @@ static __device__ __align__(256) int g_err_word[64];
 constexpr int kMaxDevices = 64;
 
 struct DeviceSetup {
-    std::once_flag once;
-    cudaError_t status = cudaSuccess;
+    bool done = false;        // set only after a set-up that succeeded
+    int major = 0, minor = 0; // compute capability of the device
     void* scratch = nullptr;  // device address of g_scratch on this device
     int* err = nullptr;       // device address of g_err_word on this device
 };
 DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
 
-// Once per device, with that device current: look up the device addresses of
-// the file-scope arrays and raise the shared-memory limit of the TMA kernels.
+// Once per device, with that device current: read its compute capability,
+// look up the device addresses of the file-scope arrays and raise the
+// shared-memory limit of the TMA kernels.  A set-up that fails is not
+// remembered: the next call on that device tries again.
 cudaError_t device_setup(int dev, DeviceSetup** out) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
     DeviceSetup& s = g_setup[dev];
-    std::call_once(s.once, [&] {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e == cudaSuccess) {
-            s.scratch = p;
-            e = cudaGetSymbolAddress(&p, g_err_word);
-        }
-        if (e == cudaSuccess) {
-            s.err = static_cast<int*>(p);
-            e = sp::prepare_kernels();
-        }
-        s.status = e;
-    });
     *out = &s;
-    return s.status;
+    if (s.done) return cudaSuccess;
+    int major = 0, minor = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (e != cudaSuccess) return e;
+    s.major = major;
+    s.minor = minor;
+    if (major < 10) return cudaSuccess;  // rejected by the caller; nothing to set up
+    void* p = nullptr;
+    void* q = nullptr;
+    if ((e = cudaGetSymbolAddress(&p, g_scratch)) != cudaSuccess) return e;
+    if ((e = cudaGetSymbolAddress(&q, g_err_word)) != cudaSuccess) return e;
+    if ((e = sp::prepare_kernels()) != cudaSuccess) return e;
+    s.scratch = p;
+    s.err = static_cast<int*>(q);
+    s.done = true;
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -92,6 +102,8 @@ extern "C" int sp_do_rk4_noalloc(const sp_params* p, const double* in, double* o
     DeviceSetup* ds = nullptr;
     if ((e = device_setup(dev, &ds)) != cudaSuccess)
         return sp_report(SP_ERR_CUDA, "sp_do_rk4_noalloc: set-up on device %d failed: %s", dev, cudaGetErrorString(e));
+    if (ds->major < 10)
+        return sp_report(SP_ERR_UNSUPPORTED, "this library is built for sm_100a (found sm_%d%d)", ds->major, ds->minor);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     double* ya = static_cast<double*>(ds->scratch);
     double* yb = ya + g.total;

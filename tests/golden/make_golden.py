@@ -1,7 +1,11 @@
 """Generates the golden fixtures under tests/golden/ from the reference.
 
-Run in a container where the reference tree is mounted (its path is the first
-argument, default /root/reference).  Two fixture files come out:
+Run in a container where the reference tree is mounted; its path is the one
+required argument:
+
+    python tests/golden/make_golden.py <path-to-the-reference-checkout>
+
+Two fixture files come out:
 
 * ``result_dat.json`` -- the Parareal convergence table that the reference
   committed (jobs/paperJobs/01-Convergence/result.dat:1-6): max-norm relative
@@ -12,17 +16,17 @@ argument, default /root/reference).  Two fixture files come out:
   reference's own Python implementation (py/Convection.py:12-36,
   Convection.getExact / getSolution) at a few grids and times.
 """
+import argparse
 import importlib.util
 import json
 import os
-import sys
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def main(ref="/root/reference"):
+def main(ref):
     rows = []
     with open(os.path.join(ref, "jobs/paperJobs/01-Convergence/result.dat")) as f:
         for line in f:
@@ -54,4 +58,6 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("reference", help="root of the andyspiros/StencilParareal checkout")
+    main(ap.parse_args().reference)

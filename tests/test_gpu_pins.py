@@ -1,0 +1,135 @@
+"""Parity at the benchmarked configurations.
+
+* The fine-propagator workload at full size (256^3 FP64, c = (1, 0.5, 0.25),
+  nu = 1e-3, dt = 5e-5, the 8-mode Fourier field of seed 1) against the
+  oracle, under the launch shapes the benchmark runs: whatever the autotuner
+  picks, and the two shapes it has picked on the boxes measured (the four
+  single-stage TMA kernels with 4-row tiles and z-chunks of 8, and the fused
+  stage pairs).  52 steps cross a graph-chunk boundary (chunks of 50 steps).
+* The one-GPU Parareal workload (128^3, 32 slices, FP32 RK4 coarse, increment
+  form) and the first 96^3 instance of the 48-instance batch, at full size,
+  against oracle pins made by ``tests/golden/make_pins.py`` (the oracle needs
+  ~30 min of 8 cores for them): values at 4096 seeded cells, whole-field sums,
+  and the oracle's per-iteration errors and defects, for both stopping rules
+  the benchmark reports.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from ics import fourier_modes, gaussian_noise, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12   # FP64 propagator vs the oracle, relative L2
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+N2, DT2, STEPS2 = 256, 5e-5, 52
+
+
+@pytest.fixture(scope="module")
+def ref256(orc):
+    q0 = fourier_modes(N2, seed=1)
+    p = orc.params(N2, dx=1.0 / N2, nu0=1e-3, cx=1.0, cy=0.5, cz=0.25)
+    orc.set_threads(os.cpu_count() or 1)
+    try:
+        ref = orc.rk4(p, q0, 0.0, DT2, STEPS2)
+    finally:
+        orc.set_threads(min(4, os.cpu_count() or 1))
+    return q0, ref
+
+
+def _conv256(sp):
+    return sp.Convection(N2, N2, N2, 1.0 / N2, 1e-3, 0.0, 1.0, 0.5, 0.25)
+
+
+@pytest.mark.parametrize("tune", ["auto", (4, 8, 1), (8, 0, 2)], ids=["autotuned", "stages_ty4_z8", "pairs_ty8"])
+def test_fine_workload_256cube_matches_oracle(sp, ref256, tune):
+    q0, ref = ref256
+    conv = _conv256(sp)
+    if tune == "auto":
+        conv.autotune(sp.SP_F64, 1)
+    else:
+        conv.set_tune(sp.SP_F64, 1, *tune)
+    fin, fout = conv.field(), conv.field()
+    conv.upload(fin, q0)
+    conv.DoRK4(fin, fout, 0.0, DT2, STEPS2)
+    assert rel_l2(conv.download(fout), ref) < TOL64
+
+
+def test_fine_workload_256cube_host_buffers_match_oracle(sp, ref256):
+    """The benchmark's end-to-end call: sp_do_rk4_host, dense host arrays in and out."""
+    q0, ref = ref256
+    conv = _conv256(sp)
+    conv.autotune(sp.SP_F64, 1)
+    assert rel_l2(conv.DoRK4Host(q0, 0.0, DT2, STEPS2), ref) < TOL64
+
+
+def _pin(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def _sample(conv, f, pin):
+    q = conv.download(f)
+    return q.reshape(-1)[pin["sample_index"]], np.array([q.sum(), (q * q).sum()])
+
+
+def _check_field(conv, f, pin, key, tol):
+    s, m = _sample(conv, f, pin)
+    assert rel_l2(s, pin[key + "_sample"]) < tol, key
+    assert np.allclose(m, pin[key + "_moments"], rtol=max(tol, 1e-12), atol=0), (key, m, pin[key + "_moments"])
+
+
+def _run_pinned_parareal(sp, name, tune_like_batch):
+    pin = _pin(name)
+    n, P = int(pin["n"]), int(pin["P"])
+    c = [float(v) for v in pin["c"]]
+    nu0 = float(pin["nu0"])
+    conv = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, *c)
+    if tune_like_batch:
+        # the batch benchmark's tuning: the batched tune of 16 fields applied to P
+        a64 = conv.autotune(sp.SP_F64, 16)
+        t64 = a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"]
+        t32 = conv.autotune(sp.SP_F32, 1)["S2"]
+        conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
+        conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
+    else:
+        # the one-GPU Parareal benchmark's tuning
+        conv.autotune(sp.SP_F64, 1)
+        conv.autotune(sp.SP_F64, P)
+        conv.autotune(sp.SP_F32, 1)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, gridSize=n, endTime=float(pin["T"]),
+                                   timeStepsFine=int(pin["timeStepsFine"]), timeStepsCoarse=int(pin["timeStepsCoarse"]),
+                                   kmax=8)
+    f0, fs, fq = conv.field(), conv.field(), conv.field()
+    conv.upload(f0, gaussian_noise(n, seed=int(pin["seed"])))
+    sp.Parareal(conv, f0, fs, 0.0, conf).DoSerial()
+    _check_field(conv, fs, pin, "serial", TOL64)
+    err_l2, defect = pin["err_l2"], pin["defect"]
+    # the two stopping rules of the benchmark: the error against the serial fine
+    # solution (the configuration's criterion), and the defect between iterations
+    k_ref = int(np.argmax(err_l2 < 1e-8)) + 1
+    k_def = int(np.argmax(defect < 1e-8)) + 1
+    assert err_l2[k_ref - 1] < 1e-8 and defect[k_def - 1] < 1e-8, (err_l2, defect)
+    for rule, k_expect in (("reference", k_ref), ("defect", k_def)):
+        par = sp.Parareal(conv, f0, fq, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=1e-8, tol_kind=rule)
+        rep = par.DoParallel(reference=fs)
+        assert rep["iterations"] == k_expect, (rule, rep["iterations"], k_expect)
+        # FP32 G acts on the FP64 increment only: its rounding differs from the
+        # oracle's literal FP32 order far below the 1e-8 target
+        _check_field(conv, fq, pin, f"iter{k_expect}", 1e-9)
+        for k in range(k_expect):
+            assert abs(rep["err_l2"][k] - err_l2[k]) <= 0.05 * err_l2[k] + 1e-13, (rule, k, rep["err_l2"], err_l2)
+            assert abs(rep["defect"][k] - defect[k]) <= 0.05 * defect[k] + 1e-13, (rule, k, rep["defect"], defect)
+    return pin
+
+
+def test_parareal_workload_128cube_P32_matches_oracle_pin(sp):
+    pin = _run_pinned_parareal(sp, "pin_parareal_128cube_P32", tune_like_batch=False)
+    assert int(pin["n"]) == 128 and int(pin["P"]) == 32
+
+
+def test_batch_instance_96cube_matches_oracle_pin(sp):
+    pin = _run_pinned_parareal(sp, "pin_parareal_96cube_P12", tune_like_batch=True)
+    assert int(pin["n"]) == 96 and int(pin["P"]) == 12
