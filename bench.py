@@ -18,9 +18,14 @@ region.
 (oracle/, the reference itself needs Boost and MPI and cannot be built here)
 on the host cores on a bounded sample of the same workload.
 
-Launch: python bench.py [--gpus N --steps K --warmup W]; N>1 under torchrun
-(one independent replica per GPU: the propagator does not shard, "weak"
-scaling with no collective on the data path).
+Launch: python bench.py [--gpus N --steps K --warmup W]; N>1 under torchrun.
+The headline value at N>1 is N independent replicas of the fine-propagator
+step (the propagator does not shard: "weak" scaling with no collective on
+its data path).  At N>1 the line also carries `parareal_pipeline`: the
+one-GPU Parareal workload run as the reference's slice pipeline over all N
+ranks (DistributedParareal: NCCL send/recv of one field per iteration and
+rank boundary), timed on the device (max over ranks) beside the same problem
+on one GPU.
 """
 from __future__ import annotations
 
@@ -341,6 +346,73 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
     return out
 
 
+def pipeline_summary(torch, sp, dist, rank, world, device, n=128, P=32):
+    """The Parareal slice pipeline over the ranks of the process group (one GPU
+    each): the one-GPU Parareal workload (n^3, P slices, T=0.2, fine RK4 FP64
+    dt=1e-5, coarse RK4 FP32, increment form), rank r holding the slice window
+    slice_bounds(P, world, r); per iteration every rank runs its batched fine
+    sweep, receives the previous rank's boundary field (NCCL recv into its own
+    HBM), runs its coarse sweep and corrections and sends its boundary field on
+    (the reference's MPI ring, Parareal.h:116-165), stopping once the defect
+    over all ranks is below 1e-8.  Time: CUDA events on each rank's library
+    stream, max over ranks.  Rank 0 also times the same problem on its GPU
+    alone (DoParallel, same stopping rule) for comparison."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ics import gaussian_noise
+    from stencilparareal_b200.parareal import DistributedParareal, WindowParareal, slice_bounds
+    T, tsF, tsC, tol = 0.2, 20000, 200, 1e-8
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+    lo, hi = slice_bounds(P, world, rank)
+    conv.autotune(sp.SP_F64, 1)
+    conv.autotune(sp.SP_F64, hi - lo)
+    conv.autotune(sp.SP_F32, 1)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.01, gridSize=n, endTime=T, timeStepsFine=tsF,
+                                   timeStepsCoarse=tsC, kmax=8)
+    f0, fs, fref = conv.field(), conv.field(), conv.field()
+    conv.upload(f0, gaussian_noise(n, seed=0))
+    last = rank == world - 1
+    if last:  # the serial fine solution, for the error of the result
+        sp.Parareal(conv, f0, fref, 0.0, conf).DoSerial()
+    w = WindowParareal(conv, f0, fs, 0.0, conf, lo, hi - lo, coarse="rk4", coarse_precision="f32")
+    dp = DistributedParareal(w)
+    dp.run(8, tol)  # warm: graph capture, communicator set-up
+    conv.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(conv.stream)
+    its, defects = dp.run(8, tol)
+    e1.record(conv.stream)
+    conv.synchronize()
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) * 1e-3
+    err = conv.errors(w.boundary, fref)[1] if last else 0.0
+    t = torch.tensor([secs, err], dtype=torch.float64, device=f"cuda:{device}" if dist.get_backend() == "nccl"
+                     else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    secs_max, err_last = float(t[0]), float(t[1])
+    one_gpu_s = None
+    if rank == 0:
+        # the same problem on this GPU alone, for comparison
+        c1 = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+        c1.autotune(sp.SP_F64, P)
+        c1.autotune(sp.SP_F32, 1)
+        g0, g1 = c1.field(), c1.field()
+        c1.upload(g0, gaussian_noise(n, seed=0))
+        par = sp.Parareal(c1, g0, g1, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=tol, tol_kind="defect")
+        par.DoParallel()
+        one_gpu_s = par.DoParallel()["seconds"]
+    dist.barrier()
+    return {"config": f"{n}^3, P={P}, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (200 rounded up to a multiple "
+                      f"of P), increment form, Gaussian+noise IC seed 0, c=(1,1,1), nu=0.01; slice windows "
+                      f"{[slice_bounds(P, world, r) for r in range(world)]}",
+            "ranks": world, "exchange": f"torch.distributed {dist.get_backend()} send/recv of one FP64 field "
+                                        f"per iteration and rank boundary, MAX all-reduce of the defect",
+            "stop_rule": "defect < 1e-8 (max over ranks)", "iterations": its, "defects": defects,
+            "seconds": secs_max, "err_l2_vs_serial": err_last, "one_gpu_parareal_s": one_gpu_s,
+            "speedup_vs_one_gpu": one_gpu_s / secs_max if one_gpu_s else None}
+
+
 def adjoint_summary(torch, sp, device):
     """Adjoint: gradient of 0.5||q(T)-q_target||^2 through 400 RK4 FP64 steps at 128^3, checkpoint 20."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -380,6 +452,13 @@ def main():
     ap.add_argument("--tune", default="auto", help="'auto' or ty,zchunk,kind for the stage kernels")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: one 256^3 DoRK4 of 2 steps with the given --tune, no timing")
+    ap.add_argument("--no-pipeline", action="store_true", help="N>1: skip the Parareal slice pipeline")
+    ap.add_argument("--pipeline-only", action="store_true",
+                    help="N>1: run only the Parareal slice pipeline (prints its JSON object)")
+    ap.add_argument("--pipeline-grid", type=int, default=128)
+    ap.add_argument("--pipeline-slices", type=int, default=32)
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend for N>1 (gloo: exchange through host memory)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,13 +472,20 @@ def main():
     spbuild.build()
 
     dist = None
+    device = local % max(torch.cuda.device_count(), 1)
+    torch.cuda.set_device(device)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    device = local
-    torch.cuda.set_device(device)
+        kw = {"device_id": torch.device(f"cuda:{device}")} if args.dist_backend == "nccl" else {}
+        dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120), **kw)
+        if args.pipeline_only:
+            out = pipeline_summary(torch, sp, dist, rank, world, device, args.pipeline_grid, args.pipeline_slices)
+            if rank == 0:
+                print(json.dumps({"parareal_pipeline": out}), flush=True)
+            dist.barrier()
+            dist.destroy_process_group()
+            return 0
     n = N_FINE
     conv = sp.Convection(n, n, n, 1.0 / n, NU, 0.0, C[0], C[1], C[2], device=device)
     if args.tune == "auto" and not args.profile:
@@ -508,7 +594,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (each 256^3 FP64 field is 134 MB)",
-                       "parallelism": f"replicas x{world}", "tune": tune},
+                       "parallelism": f"replicas x{world}" + (", Parareal slice pipeline over "
+                                                              f"{args.dist_backend}" if world > 1 else ""),
+                       "tune": tune},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "traffic_unit": "dram bytes per launch (ncu, profiles/traffic.json)",
@@ -540,6 +628,10 @@ def main():
                                                       line.get("parareal", {}).get("serial_fine_s"))
             except Exception as ex:  # reported, not hidden
                 line["cpu_vs_gpu"] = {"error": repr(ex)}
+    if dist and not args.no_pipeline:
+        # every rank takes part: the Parareal slice pipeline over the process group
+        line["parareal_pipeline"] = pipeline_summary(torch, sp, dist, rank, world, device, args.pipeline_grid,
+                                                     args.pipeline_slices)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -176,17 +176,29 @@ int sp_parareal_destroy(sp_parareal* pr);
  * runs of all slices batched per RK stage, coarse sweep slice by slice, the
  * correction U = G(new) + F(old) - G(old) fused with the defect norms.
  * `initial` and `solution` are FP64 fields; `reference` (may be NULL) is the
- * serial fine solution used for err_l2/err_max and for SP_TOL_REFERENCE. */
+ * serial fine solution used for err_l2/err_max and for SP_TOL_REFERENCE.
+ * All iterations run in one CUDA-graph launch: a conditional WHILE node repeats
+ * the iteration, and a kernel at its end evaluates the defect (and the error
+ * against `reference`) and decides on the device whether to go on (kmax, the
+ * tolerance, a non-finite defect); the host synchronises once, at the end.  The
+ * reference's loop is the same with a fixed kmax (Parareal.h:116). */
 int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solution,
                             const double* reference, sp_parareal_report* report);
+/* Measurement switch, no counterpart in the reference: host_loop = 1 runs
+ * DoParallel as one graph launch per iteration with the stopping test on the
+ * host (a device-to-host copy and a synchronisation per iteration); 0 (the
+ * default) as one launch for all iterations.  Both give identical fields. */
+int sp_parareal_set_host_loop(sp_parareal* pr, int host_loop);
 /* Parareal::DoSerial (Parareal.h:250-253): DoRK4(initial, solution, 0, dtF, tsF*P). */
 int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution);
 
 /* Many independent Parareal solves at once (grids, parameters, slice counts and
  * step counts may all differ; all handles on one device).  Each instance's
- * iteration (batched fine sweep + coarse sweep) is a child graph of one CUDA
- * graph, launched once per iteration; converged instances are gated off on the
- * device.  This replaces running the reference's MPI job once per instance.
+ * iteration (batched fine sweep + coarse sweep) is a child graph; the children
+ * run concurrently inside one conditional WHILE node, so the predictors
+ * aside the whole run is one graph launch; converged instances are gated off
+ * on the device.  This replaces running the reference's MPI job once per
+ * instance.
  * run: initial[i], solution[i] (and reference[i], may be NULL) are FP64 fields of
  * instance i; reports[i] (may be NULL) as for sp_parareal_do_parallel; *seconds
  * gets the device time of the whole run. */
@@ -195,6 +207,11 @@ int sp_parareal_batch_create(sp_parareal* const* instances, int n, sp_parareal_b
 int sp_parareal_batch_destroy(sp_parareal_batch* b);
 int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* initial, double* const* solution,
                           const double* const* reference, sp_parareal_report* reports, double* seconds);
+/* As sp_parareal_set_host_loop, for a batch: 0 (default) runs every iteration of
+ * every instance in one graph launch (a conditional WHILE node around the
+ * instances' iteration graphs; instances that are done are gated off on the
+ * device), 1 one launch and one host synchronisation per iteration. */
+int sp_parareal_batch_set_host_loop(sp_parareal_batch* b, int host_loop);
 
 /* Slice-window steps for a Parareal spread over several GPUs (the reference's
  * one-rank-per-slice MPI ring, Parareal.h:110-171, with one rank per slice

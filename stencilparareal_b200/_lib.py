@@ -93,6 +93,7 @@ _SIGS = {
     "sp_parareal_destroy": (_i, [_vp]),
     "sp_parareal_do_parallel": (_i, [_vp, _vp, _vp, _vp, C.POINTER(SpPararealReport)]),
     "sp_parareal_do_serial": (_i, [_vp, _vp, _vp]),
+    "sp_parareal_set_host_loop": (_i, [_vp, _i]),
     "sp_adjoint_rk4": (_i, [_vp, _vp, _vp, _vp, _d, _d, _i, _i, C.POINTER(_d), _vp, C.POINTER(_d)]),
     "sp_last_error": (C.c_char_p, []),
     "sp_abi_version": (_i, []),
@@ -109,6 +110,7 @@ _SIGS = {
     "sp_parareal_window_coarse": (_i, [_vp, _i, _vp, _vp, C.POINTER(_d)]),
     "sp_parareal_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "sp_parareal_batch_destroy": (_i, [_vp]),
+    "sp_parareal_batch_set_host_loop": (_i, [_vp, _i]),
     "sp_parareal_batch_run": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
                                    C.POINTER(SpPararealReport), C.POINTER(_d)]),
 }

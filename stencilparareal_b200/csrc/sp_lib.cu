@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -967,6 +968,118 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
 
 // ---------------------------------------------------------------------------
 // Parareal.
+
+namespace {
+
+// Device state of an iteration loop that runs inside one graph launch: a
+// conditional WHILE node repeats the iteration body; the body's last kernel
+// turns the per-slice defect sums into the iteration's defect (and errors
+// against the reference), records them and sets the loop condition.
+struct LoopCtl {
+    int k;                           // iterations done in this run
+    int nonfinite;                   // 1: a defect sum was not finite (the loop stopped there)
+    int stopped;                     // batch: this instance no longer iterates
+    int pad;
+    unsigned long long t_head, t_mid;
+    unsigned long long ns_fine, ns_coarse;  // %globaltimer time of the fine / coarse sweeps
+    double defect[SP_MAX_ITERS];
+    double err_l2[SP_MAX_ITERS];
+    double err_max[SP_MAX_ITERS];
+};
+
+struct LoopArgs {
+    LoopCtl* c;
+    int* item_lo;
+    const double* def;   // 2P defect sums
+    const double* err4;  // error sums against the reference
+    int P, skip, kmax, tol_kind, has_ref;
+    double tol;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Iteration k's first slice still iterating: slices < k are exact after k iterations.
+__device__ __forceinline__ int loop_lo(const LoopArgs& a, int k) { return a.skip ? min(k, a.P) : 0; }
+
+__global__ void k_loop_head(LoopArgs a) {
+    a.c->t_head = global_ns();
+    *a.item_lo = loop_lo(a, a.c->k);
+}
+
+__global__ void k_loop_mid(LoopCtl* c) { c->t_mid = global_ns(); }
+
+// The host loop's per-iteration decision (sp_parareal_do_parallel), on the
+// device: defect = max over iterating slices of sqrt(sum (U+ - U)^2 / sum U+^2).
+// Returns whether the instance iterates again.
+__device__ bool loop_decide(const LoopArgs& a) {
+    LoopCtl* c = a.c;
+    const unsigned long long t = global_ns();
+    c->ns_fine += c->t_mid - c->t_head;
+    c->ns_coarse += t - c->t_mid;
+    const int k = c->k;
+    double defect = 0.;
+    bool finite = true;
+    for (int r = loop_lo(a, k); r < a.P; ++r) {
+        const double num = a.def[2 * r], den = a.def[2 * r + 1];
+        if (!isfinite(num) || !isfinite(den)) finite = false;
+        if (den > 0) defect = fmax(defect, sqrt(num / den));
+    }
+    double el2 = 0., emax = 0.;
+    if (a.has_ref) {
+        el2 = sqrt(a.err4[0] / a.err4[1]);
+        emax = a.err4[2] / a.err4[3];
+    }
+    c->defect[k] = defect;
+    c->err_l2[k] = el2;
+    c->err_max[k] = emax;
+    c->k = k + 1;
+    bool cont = finite && k + 1 < a.kmax;
+    if (!finite) c->nonfinite = 1;
+    if (a.tol_kind == SP_TOL_DEFECT && defect < a.tol) cont = false;
+    if (a.tol_kind == SP_TOL_REFERENCE && a.has_ref && el2 < a.tol) cont = false;
+    return cont;
+}
+
+__global__ void k_loop_tail(LoopArgs a, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, loop_decide(a) ? 1u : 0u);
+}
+
+// Batch of instances (sp_parareal_batch_run): before each iteration every
+// instance that has not stopped gets its item_lo, a stopped one item_lo = P
+// (its kernels return at once).
+__global__ void k_batch_head(const LoopArgs* a, int n) {
+    const unsigned long long t = global_ns();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        LoopCtl* c = a[i].c;
+        if (!c->stopped && c->k >= a[i].kmax) c->stopped = 1;
+        *a[i].item_lo = c->stopped ? a[i].P : loop_lo(a[i], c->k);
+        c->t_head = c->t_mid = t;
+    }
+}
+
+// After each iteration: the decision of every running instance (an instance is
+// also exact, and stops, after P iterations); the loop goes on while any runs.
+__global__ void k_batch_tail(const LoopArgs* a, int n, cudaGraphConditionalHandle h) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        LoopCtl* c = a[i].c;
+        if (c->stopped) continue;
+        const bool cont = loop_decide(a[i]) && c->k < a[i].P;
+        if (cont) atomicOr(&any, 1);
+        else c->stopped = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+}  // namespace
+
 struct sp_parareal {
     sp_convection* prop = nullptr;
     sp_parareal_cfg cfg{};
@@ -991,10 +1104,18 @@ struct sp_parareal {
     double* h_def = nullptr;   // pinned, 2P + 4
     cudaGraphExec_t iter = nullptr;
     long long iter_nodes = 0;
+    cudaGraphExec_t loop = nullptr;      // all iterations in one launch (conditional WHILE node)
+    const double* loop_ref = nullptr;    // reference field the loop graph was captured with
+    long long loop_nodes = 0;            // kernel launches of one loop iteration
+    DevBuf lctl;                         // LoopCtl
+    LoopCtl* h_lctl = nullptr;           // pinned copy
+    int host_loop = 0;                   // 1: one graph launch and one host sync per iteration
     int coarse_res = 0;    // which Gt buffer holds the coarse result after a sweep step
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     ~sp_parareal() {
         if (iter) cudaGraphExecDestroy(iter);
+        if (loop) cudaGraphExecDestroy(loop);
+        if (h_lctl) cudaFreeHost(h_lctl);
         if (wfine) cudaGraphExecDestroy(wfine);
         if (wcoarse) cudaGraphExecDestroy(wcoarse);
         if (h_itemlo) cudaFreeHost(h_itemlo);
@@ -1054,28 +1175,47 @@ int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0,
 // parts: 1 = F sweep, 2 = G sweep, 3 = both.  zero_min: in the increment form the
 // G sweep zeroes the increment of its first iterating slice unless that is a slice
 // below zero_min (a window's slice 0 gets its increment from the previous window).
-int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long* nodes_out, int parts = 3,
-                      int zero_min = 0) {
+bool fused_sweep(const sp_parareal* pr) {
     sp_convection* h = pr->prop;
-    cudaStream_t s = h->stream();
+    return h->P.nufreq == 0. && h->tune(0, pr->P).fused && pair_supported(h->g4);
+}
+
+// Allocates the fine-sweep scratch of the path the tune selects; must run
+// before a capture of the iteration.
+int prepare_iteration(sp_parareal* pr, int parts) {
+    if (!(parts & 1)) return SP_OK;
+    const int P = pr->P;
+    const Geo& g = pr->g64;
+    const Geo& g4 = pr->prop->g4;
+    if ((fused_sweep(pr) ? pr->fw.alloc((size_t)3 * P * g4.total * g4.es)
+                         : pr->fs.alloc((size_t)3 * P * g.total * g.es)) != cudaSuccess)
+        return fail(SP_ERR_NOMEM, "fine-sweep scratch for %d slices", P);
+    return SP_OK;
+}
+
+// Enqueues one Parareal iteration (Parareal.h:116-165 for every slice) on s,
+// which is being captured:
+//   F sweep   : tsF RK4 steps of all slices r >= item_lo, batched per stage
+//   G sweep   : for r = item_lo..P-1: G(U_r) (coarse), correction into U_{r+1}
+// parts: 1 = F sweep, 2 = G sweep, 3 = both.  zero_min: in the increment form the
+// G sweep zeroes the increment of its first iterating slice unless that is a slice
+// below zero_min (a window's slice 0 gets its increment from the previous window).
+// mid (may be null): a kernel enqueued between the two sweeps.
+int emit_iteration(sp_parareal* pr, cudaStream_t s, bool events, int parts, int zero_min,
+                   const std::function<cudaError_t()>& mid = nullptr) {
+    sp_convection* h = pr->prop;
     const int P = pr->P;
     const Geo& g = pr->g64;
     const Tune tf = h->tune(0, P);
     int* err = h->err.as<int>();
     const bool const_nu = h->P.nufreq == 0.;
-    // F sweep as fused stage pairs when the tune says so and one nu serves all
-    // slices; scratch for the chosen path, allocated before the capture
-    const bool fused = const_nu && tf.fused && pair_supported(h->g4);
+    // F sweep as fused stage pairs when the tune says so and one nu serves all slices
+    const bool fused = fused_sweep(pr);
     const Geo& g4 = h->g4;
-    if ((parts & 1) && (fused ? pr->fw.alloc((size_t)3 * P * g4.total * g4.es)
-                              : pr->fs.alloc((size_t)3 * P * g.total * g.es)) != cudaSuccess)
-        return fail(SP_ERR_NOMEM, "fine-sweep scratch for %d slices", P);
     const size_t fstride = (size_t)P * g.total;
     double* ya = pr->fs.as<double>();
     double* yb = ya + fstride;
     double* acc = yb + fstride;
-    SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    const long long before = launches();
     int rc = SP_OK;
     cudaError_t e = events ? cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal) : cudaSuccess;
     if (fused && (parts & 1)) {
@@ -1110,6 +1250,7 @@ int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long*
         e = enqueue_rk4_step(g, 0, h->coef, pr->dtF, nu, in, pr->f(0), ya, yb, acc, P, pr->itemlo(), 0, tf, s, err);
     }
     if (e == cudaSuccess && events) e = cudaEventRecordWithFlags(pr->ev[1], s, cudaEventRecordExternal);
+    if (e == cudaSuccess && mid) e = mid();
     if (e == cudaSuccess && (parts & 2)) e = cudaMemsetAsync(pr->def(), 0, 2 * P * sizeof(double), s);
     const bool delta = pr->cfg.coarse_delta != 0;
     // increment form: the first slice still iterating receives an unchanged input
@@ -1130,14 +1271,27 @@ int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long*
         }
     }
     if (e == cudaSuccess && rc == SP_OK && events) e = cudaEventRecordWithFlags(pr->ev[2], s, cudaEventRecordExternal);
+    if (rc != SP_OK) return rc;
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, "iteration capture: %s", cudaGetErrorString(e));
+    return SP_OK;
+}
+
+// Captures one Parareal iteration (emit_iteration) into a new graph.
+int capture_iteration(sp_parareal* pr, bool events, cudaGraph_t* out, long long* nodes_out, int parts = 3,
+                      int zero_min = 0) {
+    cudaStream_t s = pr->prop->stream();
+    int rc = prepare_iteration(pr, parts);
+    if (rc) return rc;
+    SP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const long long before = launches();
+    rc = emit_iteration(pr, s, events, parts, zero_min);
     const long long nodes = launches() - before;
     add_launches(-nodes);
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(s, &graph);
-    if (rc != SP_OK || e != cudaSuccess) {
+    if (rc != SP_OK) {
         if (graph) cudaGraphDestroy(graph);
-        if (rc != SP_OK) return rc;
-        return fail(SP_ERR_CUDA, "iteration capture: %s", cudaGetErrorString(e));
+        return rc;
     }
     if (e2 != cudaSuccess) return fail(SP_ERR_CUDA, "iteration end capture: %s", cudaGetErrorString(e2));
     *out = graph;
@@ -1154,6 +1308,97 @@ int build_iteration_graph(sp_parareal* pr) {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, "iteration instantiate: %s", cudaGetErrorString(e));
     pr->iter_nodes = nodes;
+    return SP_OK;
+}
+
+LoopArgs loop_args(sp_parareal* pr, const double* reference) {
+    LoopArgs a;
+    a.c = pr->lctl.as<LoopCtl>();
+    a.item_lo = pr->itemlo();
+    a.def = pr->def();
+    a.err4 = pr->err4();
+    a.P = pr->P;
+    a.skip = pr->cfg.skip_converged ? 1 : 0;
+    a.kmax = pr->cfg.kmax;
+    a.tol_kind = pr->cfg.tol_kind;
+    a.has_ref = reference ? 1 : 0;
+    a.tol = pr->cfg.tol;
+    return a;
+}
+
+// Every iteration of DoParallel (Parareal.h:116-165) in one graph: a
+// conditional WHILE node whose body is k_loop_head (item_lo from the device
+// iteration counter), the iteration, the errors against `reference` (if any)
+// and k_loop_tail, which records the defect and decides on the device whether
+// to iterate again (the host loop's test: kmax, the tolerance, non-finite
+// defects).  Rebuilt when the reference field changes.
+int build_loop_graph(sp_parareal* pr, const double* reference) {
+    if (pr->loop && pr->loop_ref == reference) return SP_OK;
+    if (pr->loop) {
+        cudaGraphExecDestroy(pr->loop);
+        pr->loop = nullptr;
+    }
+    int rc = prepare_iteration(pr, 3);
+    if (rc) return rc;
+    if (pr->lctl.alloc(sizeof(LoopCtl)) != cudaSuccess) return fail(SP_ERR_NOMEM, "loop control");
+    if (!pr->h_lctl) SP_CUDA(cudaMallocHost(&pr->h_lctl, sizeof(LoopCtl)));
+    cudaStream_t s = pr->prop->stream();
+    const LoopArgs a = loop_args(pr, reference);
+    cudaGraph_t g = nullptr;
+    SP_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hc;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hc;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(SP_ERR_CUDA, "loop graph: %s", cudaGetErrorString(e));
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(SP_ERR_CUDA, "loop capture: %s", cudaGetErrorString(e));
+    }
+    const long long before = launches();
+    k_loop_head<<<1, 1, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        rc = emit_iteration(pr, s, false, 3, 0, [&]() -> cudaError_t {
+            k_loop_mid<<<1, 1, 0, s>>>(a.c);
+            return cudaGetLastError();
+        });
+    }
+    if (e == cudaSuccess && rc == SP_OK && reference) {
+        e = cudaMemsetAsync(pr->err4(), 0, 4 * sizeof(double), s);
+        if (e == cudaSuccess) e = launch_errors(pr->g64, pr->u(pr->P), reference, pr->err4(), s);
+    }
+    if (e == cudaSuccess && rc == SP_OK) {
+        k_loop_tail<<<1, 1, 0, s>>>(a, hc);
+        e = cudaGetLastError();
+    }
+    const long long nodes = launches() - before + 3;  // + head, mid and tail
+    add_launches(-(launches() - before));
+    cudaGraph_t captured = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &captured);
+    if (rc != SP_OK || e != cudaSuccess || e2 != cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (rc != SP_OK) return rc;
+        return fail(SP_ERR_CUDA, "loop capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    e = cudaGraphInstantiate(&pr->loop, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        pr->loop = nullptr;
+        return fail(SP_ERR_CUDA, "loop instantiate: %s", cudaGetErrorString(e));
+    }
+    pr->loop_ref = reference;
+    pr->loop_nodes = nodes;
     return SP_OK;
 }
 
@@ -1280,6 +1525,12 @@ int sp_parareal_destroy(sp_parareal* pr) {
     return SP_OK;
 }
 
+int sp_parareal_set_host_loop(sp_parareal* pr, int host_loop) {
+    if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
+    pr->host_loop = host_loop ? 1 : 0;
+    return SP_OK;
+}
+
 int sp_parareal_do_serial(sp_parareal* pr, const double* initial, double* solution) {
     NvtxRange range("Parareal::DoSerial");
     if (!pr) return fail(SP_ERR_INVALID, "null Parareal handle");
@@ -1306,7 +1557,11 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
         rep->tsFine = pr->tsF; rep->tsCoarse = pr->tsC;
         rep->dtFine = pr->dtF; rep->dtCoarse = pr->dtC; rep->timeSliceSize = pr->slice;
     }
-    if (!pr->iter && (rc = build_iteration_graph(pr))) return rc;
+    if (pr->host_loop) {
+        if (!pr->iter && (rc = build_iteration_graph(pr))) return rc;
+    } else if (pr->cfg.kmax > 0 && (rc = build_loop_graph(pr, reference))) {
+        return rc;
+    }
 
     NvtxRange range("Parareal::DoParallel");
     SP_CUDA(cudaEventRecord(pr->ev[3], s));
@@ -1319,7 +1574,16 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     double t_f = 0., t_c = 0.;
     long long fine_cu = 0;
     const long long cells = (long long)g.ni * g.nj * g.nk;
-    for (; k < pr->cfg.kmax; ++k) {
+    const bool device_loop = !pr->host_loop && pr->cfg.kmax > 0;
+    if (device_loop) {
+        // all iterations in one graph launch; the stopping test runs on the
+        // device, and the host reads the loop's record once, after the run
+        NvtxRange it("iterations (one launch)");
+        SP_CUDA(cudaMemsetAsync(pr->lctl.p, 0, sizeof(LoopCtl), s));
+        SP_CUDA(cudaGraphLaunch(pr->loop, s));
+        SP_CUDA(cudaMemcpyAsync(pr->h_lctl, pr->lctl.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, s));
+    }
+    for (; pr->host_loop && k < pr->cfg.kmax; ++k) {
         char label[32];
         std::snprintf(label, sizeof label, "iteration %d", k + 1);
         NvtxRange it(label);
@@ -1370,6 +1634,26 @@ int sp_parareal_do_parallel(sp_parareal* pr, const double* initial, double* solu
     SP_CUDA(cudaEventSynchronize(pr->ev[4]));
     float ms = 0;
     cudaEventElapsedTime(&ms, pr->ev[3], pr->ev[4]);
+    if (device_loop) {
+        const LoopCtl& c = *pr->h_lctl;
+        k = c.k;
+        add_launches((long long)k * pr->loop_nodes);
+        for (int i = 0; i < k; ++i) {
+            const int lo = pr->cfg.skip_converged ? std::min(i, P) : 0;
+            fine_cu += (long long)(P - lo) * pr->tsF * cells;
+            if (rep) {
+                rep->defect[i] = c.defect[i];
+                rep->err_l2[i] = c.err_l2[i];
+                rep->err_max[i] = c.err_max[i];
+            }
+        }
+        t_f = c.ns_fine * 1e-9;
+        t_c = c.ns_coarse * 1e-9;
+        if (c.nonfinite) {
+            if (rep) rep->iterations = k;
+            return fail(SP_ERR_NONFINITE, "Parareal defect is not finite at iteration %d", k);
+        }
+    }
     if (rep) {
         rep->iterations = k;
         rep->seconds = ms * 1e-3;
@@ -1518,10 +1802,19 @@ struct sp_parareal_batch {
     cudaStream_t root = nullptr;
     cudaGraphExec_t exec = nullptr;
     long long nodes = 0;
+    std::vector<cudaGraph_t> children;     // each instance's captured iteration
+    cudaGraphExec_t loop = nullptr;        // all iterations of all instances in one launch
+    std::vector<const double*> loop_refs;  // reference fields the loop graph was built with
+    long long loop_nodes = 0;
+    DevBuf args;                           // LoopArgs of every instance
+    int host_loop = 0;                     // 1: one graph launch and one host sync per iteration
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> done;
     ~sp_parareal_batch() {
         if (exec) cudaGraphExecDestroy(exec);
+        if (loop) cudaGraphExecDestroy(loop);
+        for (auto c : children)
+            if (c) cudaGraphDestroy(c);
         for (auto e : ev)
             if (e) cudaEventDestroy(e);
         for (auto e : done)
@@ -1549,14 +1842,13 @@ extern "C" int sp_parareal_batch_create(sp_parareal* const* ins, int n, sp_parar
     for (auto& e : b->done) SP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     cudaGraph_t parent = nullptr;
     SP_CUDA(cudaGraphCreate(&parent, 0));
+    b->children.resize(n, nullptr);
     for (int i = 0; i < n; ++i) {
-        cudaGraph_t child = nullptr;
         long long nodes = 0;
-        int rc = capture_iteration(b->ins[i], false, &child, &nodes);
+        int rc = capture_iteration(b->ins[i], false, &b->children[i], &nodes);
         if (rc) { cudaGraphDestroy(parent); return rc; }
         cudaGraphNode_t node;
-        cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
-        cudaGraphDestroy(child);
+        cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, b->children[i]);
         if (e != cudaSuccess) { cudaGraphDestroy(parent); return fail(SP_ERR_CUDA, "child graph: %s", cudaGetErrorString(e)); }
         b->nodes += nodes;
     }
@@ -1564,6 +1856,104 @@ extern "C" int sp_parareal_batch_create(sp_parareal* const* ins, int n, sp_parar
     cudaGraphDestroy(parent);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
     *out = b.release();
+    return SP_OK;
+}
+
+namespace {
+// Every iteration of every instance in one graph launch: a conditional WHILE
+// node whose body runs k_batch_head, the instances' iterations (child graphs,
+// concurrent), the errors against the references and k_batch_tail, which
+// records each instance's defect, stops the instances that are done and ends
+// the loop when none is left.  Rebuilt when the reference fields change.
+int build_batch_loop(sp_parareal_batch* b, const double* const* reference) {
+    const int n = (int)b->ins.size();
+    std::vector<const double*> refs(n, nullptr);
+    for (int i = 0; i < n; ++i) refs[i] = reference ? reference[i] : nullptr;
+    if (b->loop && refs == b->loop_refs) return SP_OK;
+    if (b->loop) {
+        cudaGraphExecDestroy(b->loop);
+        b->loop = nullptr;
+    }
+    std::vector<LoopArgs> hargs(n);
+    for (int i = 0; i < n; ++i) {
+        sp_parareal* pr = b->ins[i];
+        if (pr->lctl.alloc(sizeof(LoopCtl)) != cudaSuccess) return fail(SP_ERR_NOMEM, "loop control");
+        if (!pr->h_lctl) SP_CUDA(cudaMallocHost(&pr->h_lctl, sizeof(LoopCtl)));
+        hargs[i] = loop_args(pr, refs[i]);
+    }
+    if (b->args.alloc(n * sizeof(LoopArgs)) != cudaSuccess) return fail(SP_ERR_NOMEM, "loop arguments");
+    SP_CUDA(cudaMemcpy(b->args.p, hargs.data(), n * sizeof(LoopArgs), cudaMemcpyHostToDevice));
+    const LoopArgs* dargs = b->args.as<LoopArgs>();
+    cudaStream_t s = b->root;
+    cudaGraph_t g = nullptr;
+    SP_CUDA(cudaGraphCreate(&g, 0));
+    auto bail = [&](cudaError_t e, const char* what) {
+        cudaGraphDestroy(g);
+        return fail(SP_ERR_CUDA, "batch loop graph (%s): %s", what, cudaGetErrorString(e));
+    };
+    cudaGraphConditionalHandle hc;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hc;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, g, nullptr, 0, &np);
+    if (e != cudaSuccess) return bail(e, "conditional node");
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    // head
+    cudaGraph_t cap = nullptr;
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return bail(e, "head capture");
+    k_batch_head<<<1, 128, 0, s>>>(dargs, n);
+    e = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(s, &cap);
+    if (e != cudaSuccess || e2 != cudaSuccess) return bail(e != cudaSuccess ? e : e2, "head");
+    cudaGraphNode_t head = nullptr;
+    size_t count = 1;
+    e = cudaGraphGetNodes(body, &head, &count);
+    if (e != cudaSuccess || count != 1) return bail(e, "head node");
+    // the instances' iterations, concurrent
+    std::vector<cudaGraphNode_t> kids(n);
+    for (int i = 0; i < n; ++i) {
+        e = cudaGraphAddChildGraphNode(&kids[i], body, &head, 1, b->children[i]);
+        if (e != cudaSuccess) return bail(e, "child node");
+    }
+    // errors against the references, decision
+    e = cudaStreamBeginCaptureToGraph(s, body, kids.data(), nullptr, n, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return bail(e, "tail capture");
+    long long extra = 2;
+    const long long before = launches();
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        if (!refs[i]) continue;
+        sp_parareal* pr = b->ins[i];
+        e = cudaMemsetAsync(pr->err4(), 0, 4 * sizeof(double), s);
+        if (e == cudaSuccess) e = launch_errors(pr->g64, pr->u(pr->P), refs[i], pr->err4(), s);
+        ++extra;
+    }
+    if (e == cudaSuccess) {
+        k_batch_tail<<<1, 128, 0, s>>>(dargs, n, hc);
+        e = cudaGetLastError();
+    }
+    add_launches(-(launches() - before));
+    e2 = cudaStreamEndCapture(s, &cap);
+    if (e != cudaSuccess || e2 != cudaSuccess) return bail(e != cudaSuccess ? e : e2, "tail");
+    e = cudaGraphInstantiate(&b->loop, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->loop = nullptr;
+        return fail(SP_ERR_CUDA, "batch loop instantiate: %s", cudaGetErrorString(e));
+    }
+    b->loop_refs = refs;
+    b->loop_nodes = b->nodes + extra;
+    return SP_OK;
+}
+}  // namespace
+
+extern "C" int sp_parareal_batch_set_host_loop(sp_parareal_batch* b, int host_loop) {
+    if (!b) return fail(SP_ERR_INVALID, "null batch handle");
+    b->host_loop = host_loop ? 1 : 0;
     return SP_OK;
 }
 
@@ -1609,7 +1999,17 @@ extern "C" int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* 
     std::vector<char> active(n, 1);
     int kmax = 0;
     for (auto* pr : b->ins) kmax = std::max(kmax, pr->cfg.kmax);
-    for (int k = 0; k < kmax; ++k) {
+    const bool device_loop = !b->host_loop && kmax > 0;
+    if (device_loop) {
+        // every iteration of every instance in one graph launch
+        int rc = build_batch_loop(b, reference);
+        if (rc) return rc;
+        for (auto* pr : b->ins) SP_CUDA(cudaMemsetAsync(pr->lctl.p, 0, sizeof(LoopCtl), s));
+        SP_CUDA(cudaGraphLaunch(b->loop, s));
+        for (auto* pr : b->ins)
+            SP_CUDA(cudaMemcpyAsync(pr->h_lctl, pr->lctl.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, s));
+    }
+    for (int k = 0; k < kmax && !device_loop; ++k) {
         int n_active = 0;
         for (int i = 0; i < n; ++i) {
             sp_parareal* pr = b->ins[i];
@@ -1666,13 +2066,39 @@ extern "C" int sp_parareal_batch_run(sp_parareal_batch* b, const double* const* 
     for (int i = 0; i < n; ++i) {
         sp_parareal* pr = b->ins[i];
         SP_CUDA(cudaMemcpyAsync(solution[i], pr->u(pr->P), pr->g64.total * 8, cudaMemcpyDeviceToDevice, s));
-        if (reports) reports[i].iterations = iters[i];
     }
     SP_CUDA(cudaEventRecord(b->ev[1], s));
     SP_CUDA(cudaEventSynchronize(b->ev[1]));
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
     if (seconds) *seconds = ms * 1e-3;
+    if (device_loop) {
+        int kdone = 0, bad = -1;
+        for (int i = 0; i < n; ++i) {
+            sp_parareal* pr = b->ins[i];
+            const LoopCtl& c = *pr->h_lctl;
+            iters[i] = c.k;
+            kdone = std::max(kdone, c.k);
+            if (c.nonfinite && bad < 0) bad = i;
+            if (!reports) continue;
+            for (int k = 0; k < c.k; ++k) {
+                const int lo = pr->cfg.skip_converged ? std::min(k, pr->P) : 0;
+                reports[i].defect[k] = c.defect[k];
+                reports[i].err_l2[k] = c.err_l2[k];
+                reports[i].err_max[k] = c.err_max[k];
+                reports[i].fine_cell_updates +=
+                    (long long)(pr->P - lo) * pr->tsF * pr->g64.ni * pr->g64.nj * pr->g64.nk;
+            }
+        }
+        add_launches((long long)kdone * b->loop_nodes);
+        if (bad >= 0) {
+            if (reports)
+                for (int i = 0; i < n; ++i) reports[i].iterations = iters[i];
+            return fail(SP_ERR_NONFINITE, "instance %d: defect not finite at iteration %d", bad, iters[bad]);
+        }
+    }
+    if (reports)
+        for (int i = 0; i < n; ++i) reports[i].iterations = iters[i];
     for (auto* pr : b->ins) {
         int rc = sp_convection_synchronize(pr->prop);
         if (rc) return rc;

@@ -148,6 +148,12 @@ class Parareal:
                 "seconds": rep.seconds, "seconds_fine": rep.seconds_fine, "seconds_coarse": rep.seconds_coarse,
                 "fine_cell_updates": rep.fine_cell_updates}
 
+    def set_host_loop(self, host_loop: bool):
+        """Measurement switch: True runs DoParallel as one graph launch and one host
+        synchronisation per iteration, False (default) all iterations in one launch
+        with the stopping test on the device.  The fields are identical."""
+        L.check(L.lib().sp_parareal_set_host_loop(self._h, 1 if host_loop else 0))
+
     def DoSerial(self):
         """Parareal::DoSerial (Parareal.h:250-253)."""
         self.prop.call(L.lib().sp_parareal_do_serial, self._h, C.c_void_p(self.initial.ptr),
@@ -183,10 +189,10 @@ class PararealBatch:
     """Many independent Parareal solves advanced together on one GPU.
 
     Each instance keeps its own grid, PDE parameters, slice count and step
-    counts; one CUDA graph launch per iteration runs all of them (the
-    instances' iteration graphs are child graphs of one parent graph) and an
-    instance stops once its tolerance is met, its kmax is used or it is exact
-    (k = P).
+    counts; one CUDA graph launch runs every iteration of all of them (the
+    instances' iteration graphs are concurrent child graphs inside a
+    conditional WHILE node) and an instance stops, on the device, once its
+    tolerance is met, its kmax is used or it is exact (k = P).
     """
 
     def __init__(self, instances):
@@ -207,6 +213,10 @@ class PararealBatch:
             self.close()
         except Exception:
             pass
+
+    def set_host_loop(self, host_loop: bool):
+        """Measurement switch, as Parareal.set_host_loop, for the whole batch."""
+        L.check(L.lib().sp_parareal_batch_set_host_loop(self._h, 1 if host_loop else 0))
 
     def run(self, references=None):
         """Runs every instance from its `initial` into its `solution`; returns (reports, seconds)."""

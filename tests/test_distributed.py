@@ -92,7 +92,7 @@ def _gpu_rank(rank, world, port, out, spec):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("coarse,prec", [("rk4", "f32"), ("euler", "f64")])
-def test_two_processes_one_gpu_equal_single_process(sp, coarse, prec):
+def test_two_processes_one_gpu_equal_single_process(sp, orc, coarse, prec):
     n, P, kmax = 12, 5, 3
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "last.npy")
@@ -103,6 +103,36 @@ def test_two_processes_one_gpu_equal_single_process(sp, coarse, prec):
     conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.02, timeStepsFine=120,
                                    timeStepsCoarse=14, kmax=kmax)
     f0, fs = conv.field(), conv.field()
-    conv.upload(f0, gaussian_noise(n, seed=1))
+    q0 = gaussian_noise(n, seed=1)
+    conv.upload(f0, q0)
     sp.Parareal(conv, f0, fs, 0.0, conf, coarse=coarse, coarse_precision=prec).DoParallel()
     assert np.array_equal(last, conv.download(fs))
+    # and against the oracle's serial restatement of DoParallel (Parareal.h:110-171);
+    # with FP32 G the windows use the increment form, as the single-process default
+    kind = {("rk4", "f32"): orc.COARSE_RK4_F32, ("euler", "f64"): orc.COARSE_EULER_F64}[(coarse, prec)]
+    cfg = orc.parareal_cfg(0.02, P, 120, 14, kmax, coarse=kind, delta=(prec == "f32"))
+    q, qs, em, el = orc.parareal(orc.params(n, nu0=0.05, cx=1.0, cy=0.5, cz=-0.25), cfg, q0)
+    diff = float(np.sqrt(((last - q) ** 2).sum() / (q ** 2).sum()))
+    assert diff < (1e-11 if prec == "f64" else 1e-8), diff
+
+
+@pytest.mark.gpu
+def test_benchmark_slice_pipeline_two_ranks_one_gpu(sp):
+    """bench.py's N>1 Parareal slice pipeline, launched as the benchmark is (torchrun,
+    one process per rank), with the gloo backend so that both ranks can share the
+    one GPU here (the exchange goes through host memory; no kernel waits on the
+    other process).  On N GPUs the same code exchanges over NCCL."""
+    import json
+    import subprocess
+    import sys
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"), "--gpus", "2",
+           "--pipeline-only", "--dist-backend", "gloo", "--pipeline-grid", "16", "--pipeline-slices", "6"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-3000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    out = json.loads(line)["parareal_pipeline"]
+    assert out["ranks"] == 2
+    assert 1 <= out["iterations"] <= 6 and out["defects"][-1] < 1e-8
+    assert out["err_l2_vs_serial"] < 1e-8
+    assert out["seconds"] > 0 and out["one_gpu_parareal_s"] > 0

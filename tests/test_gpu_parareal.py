@@ -211,3 +211,67 @@ def test_nonfinite_defect_is_reported_and_handle_recovers(sp):
     conv2.upload(f2, gaussian_noise(n, seed=31))
     sp.Parareal(conv2, f2, s2, 0.0, good, coarse="rk4", coarse_precision="f64").DoParallel()
     assert np.array_equal(got, conv2.download(s2))
+
+
+@pytest.mark.parametrize("tol_kind,tol", [("none", 0.0), ("defect", 1e-6), ("reference", 1e-7)])
+def test_one_launch_loop_equals_host_loop(sp, tol_kind, tol):
+    """All iterations in one graph launch (conditional WHILE node, stopping test on
+    the device) give the host-driven loop's fields, iteration count, defects and
+    errors bit for bit."""
+    n, P = 16, 6
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.02, 0.0, 1.0, -0.5, 0.25)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.02, gridSize=n, endTime=0.03, timeStepsFine=240,
+                                   timeStepsCoarse=18, kmax=5)
+    fin, fref = conv.field(), conv.field()
+    conv.upload(fin, gaussian_noise(n, seed=4))
+    sp.Parareal(conv, fin, fref, 0.0, conf).DoSerial()
+    outs = []
+    for host in (True, False):
+        fsol = conv.field()
+        par = sp.Parareal(conv, fin, fsol, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=tol,
+                          tol_kind=tol_kind)
+        par.set_host_loop(host)
+        rep = par.DoParallel(reference=fref)
+        rep2 = par.DoParallel(reference=fref)  # a second run of the same graph
+        assert rep2["iterations"] == rep["iterations"] and rep2["defect"] == rep["defect"]
+        outs.append((conv.download(fsol), rep))
+    (a, ra), (b, rb) = outs
+    assert np.array_equal(a, b)
+    assert ra["iterations"] == rb["iterations"]
+    assert ra["defect"] == rb["defect"] and ra["err_l2"] == rb["err_l2"] and ra["err_max"] == rb["err_max"]
+    assert ra["fine_cell_updates"] == rb["fine_cell_updates"]
+    if tol_kind == "none":
+        assert ra["iterations"] == 5
+    else:
+        assert ra["iterations"] < 5
+
+
+def test_batch_one_launch_loop_equals_host_loop(sp):
+    from stencilparareal_b200.parareal import PararealBatch
+    specs = [(12, 0.01, (1.0, -0.5, 0.3), 4, 1e-9), (16, 0.003, (-0.7, 0.9, 0.1), 6, 1e-6),
+             (10, 0.05, (0.2, 0.2, -1.0), 3, 0.0)]
+    results = []
+    for host in (True, False):
+        inst, refs, convs = [], [], []
+        for n, nu0, c, P, tol in specs:
+            conv = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, *c)
+            conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, gridSize=n, endTime=0.01, timeStepsFine=100,
+                                           timeStepsCoarse=10, kmax=P)
+            fin, fs, fr = conv.field(), conv.field(), conv.field()
+            conv.upload(fin, gaussian_noise(n, seed=n + 1))
+            sp.Parareal(conv, fin, fr, 0.0, conf).DoSerial()
+            inst.append(sp.Parareal(conv, fin, fs, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=tol,
+                                    tol_kind="defect" if tol > 0 else "none"))
+            refs.append(fr)
+            convs.append(conv)
+        batch = PararealBatch(inst)
+        batch.set_host_loop(host)
+        reps, secs = batch.run(references=refs)
+        results.append(([c.download(p.solution) for c, p in zip(convs, inst)], reps))
+    (fa, ra), (fb, rb) = results
+    for x, y in zip(fa, fb):
+        assert np.array_equal(x, y)
+    for x, y in zip(ra, rb):
+        assert x["iterations"] == y["iterations"] and x["defect"] == y["defect"] and x["err_l2"] == y["err_l2"]
+        assert x["fine_cell_updates"] == y["fine_cell_updates"]
+    assert ra[2]["iterations"] == 3  # no tolerance: exact after P = 3 iterations
