@@ -205,13 +205,23 @@ def cpu_vs_gpu_times(torch, sp, device, gpu_serial_128_s=None):
     conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
     fi, fo = conv.field(), conv.field()
     conv.upload(fi, q0)
-    conv.DoRK4(fi, fo, 0.0, dt, steps)
-    conv.synchronize()
-    t0 = time.perf_counter()
-    conv.DoRK4(fi, fo, 0.0, dt, steps)
-    conv.synchronize()
-    gpu = time.perf_counter() - t0
-    out["serial_fine_32cube_1000_steps"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01", "cpu_s": cpu, "gpu_s": gpu}
+    gpu = {}
+    for path, kind in (("stage_kernels", (4, 8, 1)), ("autotuned", None)):
+        if kind:
+            conv.set_tune(sp.SP_F64, 1, *kind)
+        else:
+            tuned = conv.autotune(sp.SP_F64, 1)
+        conv.DoRK4(fi, fo, 0.0, dt, steps)
+        conv.synchronize()
+        t0 = time.perf_counter()
+        conv.DoRK4(fi, fo, 0.0, dt, steps)
+        conv.synchronize()
+        gpu[path] = time.perf_counter() - t0
+    out["serial_fine_32cube_1000_steps"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01",
+                                            "cpu_s": cpu, "gpu_s": gpu["autotuned"],
+                                            "gpu_s_stage_kernels": gpu["stage_kernels"],
+                                            "gpu_path": "cluster-resident" if tuned["cluster"]["kind"] == 3
+                                            else "stage kernels / fused pairs"}
     n, sample, total = 128, 200, 20000
     p = O.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
     q0 = gaussian_noise(n, seed=0)
@@ -261,12 +271,20 @@ def parareal_summary(torch, sp, device):
     for rule, pr in par.items():
         pr.DoParallel(reference=qs)  # warm (graph capture)
         rep = pr.DoParallel(reference=qs)
+        # the same run with one graph launch and one host synchronisation per
+        # iteration instead of all iterations in one launch
+        pr.set_host_loop(True)
+        pr.DoParallel(reference=qs)
+        rep_host = pr.DoParallel(reference=qs)
+        pr.set_host_loop(False)
         r = {"parareal_s": rep["seconds"], "iterations": rep["iterations"],
              "err_l2_vs_serial": rep["err_l2"][-1] if rep["err_l2"] else None,
              "defects": rep["defect"], "err_l2": rep["err_l2"],
              "speedup_vs_serial": t_serial / rep["seconds"] if rep["seconds"] else None,
              "fine_s": rep["seconds_fine"], "coarse_s": rep["seconds_coarse"],
-             "fine_gcups": rep["fine_cell_updates"] / rep["seconds_fine"] / 1e9 if rep["seconds_fine"] else None}
+             "fine_gcups": rep["fine_cell_updates"] / rep["seconds_fine"] / 1e9 if rep["seconds_fine"] else None,
+             "loop": "all iterations in one graph launch (conditional WHILE node, stopping test on the device)",
+             "host_loop_s": rep_host["seconds"], "saved_by_one_launch_s": rep_host["seconds"] - rep["seconds"]}
         if rule == "reference":
             out.update(r)  # the configuration's own criterion: the headline fields
             out["stop_rule"] = "reference: last slice within 1e-8 rel. L2 of the serial FP64 fine solution"
@@ -328,6 +346,10 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
            "tunes": {str(k): v[0] for k, v in tunes.items()}}
     for rule in ("reference", "defect"):
         batch = PararealBatch(inst[rule])
+        batch.set_host_loop(True)
+        batch.run(references=refs)
+        _, secs_host = batch.run(references=refs)
+        batch.set_host_loop(False)
         batch.run(references=refs)   # warm (first launch)
         reps, secs = batch.run(references=refs)
         fine_cu = sum(r["fine_cell_updates"] for r in reps)
@@ -335,7 +357,9 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
         errs = [r["err_l2"][-1] for r in reps]
         r = {"batch_s": secs, "speedup_vs_serial_sum": serial_s / secs if secs else None,
              "iterations_max": max(its), "iterations_mean": sum(its) / len(its),
-             "err_l2_max": max(errs), "fine_gcups": fine_cu / secs / 1e9}
+             "err_l2_max": max(errs), "fine_gcups": fine_cu / secs / 1e9,
+             "loop": "every iteration of every instance in one graph launch",
+             "host_loop_s": secs_host, "saved_by_one_launch_s": secs_host - secs}
         if rule == "reference":
             out.update(r)
             out["stop_rule"] = "reference: within 1e-8 rel. L2 of each instance's serial FP64 fine solution"

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstencilparareal.so")
 LIB_CHECKED = os.path.join(HERE, "libstencilparareal_checked.so")
-SOURCES = ["sp_kernels.cu", "sp_fused.cu", "sp_lib.cu", "sp_noalloc.cu"]
+SOURCES = ["sp_kernels.cu", "sp_fused.cu", "sp_cluster.cu", "sp_lib.cu", "sp_noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 

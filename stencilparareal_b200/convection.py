@@ -185,7 +185,8 @@ class Convection:
     # -- tuning ----------------------------------------------------------------
     def set_tune(self, precision: int, batch: int, ty: int, zchunk: int, kind: int):
         """kind: 0 direct loads, 1 TMA/mbarrier pipeline (single-stage kernels);
-        2 fused stage pairs for FP64 RK4 steps (ty 8 or 16)."""
+        2 fused stage pairs for FP64 RK4 steps (ty 8 or 16); 3 the cluster-resident
+        path for FP64 RK4 propagations of small fields (ty and zchunk unused)."""
         L.check(L.lib().sp_set_tune(self._h, precision, batch, ty, zchunk, int(kind)))
 
     def autotune(self, precision: int = L.SP_F64, batch: int = 1):
@@ -212,7 +213,7 @@ class Convection:
         return {k: float(ms[i]) for i, k in enumerate(names)}
 
     def tuned_configs(self, precision: int = L.SP_F64, batch: int = 1):
-        names = {0: "S1", 1: "S2", 2: "S3", 3: "S4", 4: "euler", 9: "P12", 10: "P34"}
+        names = {0: "S1", 1: "S2", 2: "S3", 3: "S4", 4: "euler", 9: "P12", 10: "P34", 11: "cluster"}
         return {name: self.tuned_config(precision, batch, op) for op, name in names.items()}
 
 

@@ -1,0 +1,390 @@
+// sp_cluster.cu -- many RK4 steps of a small FP64 field in one launch, the
+// field held on chip in the distributed shared memory of a thread-block
+// cluster.
+//
+// Small fields (up to ~32^3) are latency-bound on the stage kernels: an RK4
+// step of a 32^3 field is four launches of ~3.5 us, most of it pipeline fill
+// and drain.  Here one cluster of C = nk / NZ CTAs owns one field: CTA c keeps
+// planes [c*NZ, (c+1)*NZ) of the stage input in shared memory, with two halo
+// planes below and above that its z-neighbours write into it, and the step
+// start q and the accumulator of its cells in registers.  A stage reads the
+// 13-point star from shared memory (x and y wrap around inside the plane; z
+// from the halo planes), writes the next stage input into the other of two
+// shared buffers and, once all its threads are past the stage, stores its two
+// lowest / highest planes into the z-neighbours' halo planes with st.async
+// (the neighbours then start the next stage, which writes into the buffer
+// this stage read), each store counting its bytes off
+// the transaction count of the receiving CTA's mbarrier.  A CTA posts the halo
+// bytes it expects for the next stage, and waits (acquire, bounded by
+// %globaltimer) until they have landed: two neighbours per stage instead of a
+// barrier over the whole cluster, no fence and no separate arrival.  Nothing
+// goes to global memory between the first load and the last store.
+//
+// Every value is computed with the operations, and in the order, of the
+// single-stage kernels (rhs_w13 and the 13-access low-storage epilogues of
+// sp_kernels.cu), so the result equals theirs bit for bit:
+//   S1: y1 = q + dt/2 k1                 S2: y2 = q + dt/2 k2, a = q + (y1-q)/3 + dt/3 k2
+//   S3: y3 = q + dt k3                   S4: q' = a + (y3-q)/3 + dt/6 k4
+// (src/Convection/Convection.cpp:318-370 in low-storage form).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "sp_device.cuh"
+#include "sp_internal.h"
+#include "sp_stencil.cuh"
+
+namespace sp {
+
+namespace {
+
+using V2 = Vec<double, 2>;
+constexpr int kClusterThreads = 512;
+
+struct ClusterArgs {
+    const double* in;       // caller layout, items fields back to back
+    double* out;
+    long long item_stride, origin, px, plane;
+    int ni, nj, nk;
+    int nsteps;
+    const W13<double>* wtab;  // per-step weights (nu(t) varies) or null
+    W13<double> w;            // weights of every step when wtab is null
+    double dthalf, dt, dt3, dt6;
+    const int* item_lo;
+    int item_base;
+    int* err;
+    StoreBounds sb;
+};
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+// All threads of all CTAs of the cluster (hardware barrier, like __syncthreads).
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Shared-memory address of the same variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+// 16 bytes into another CTA's shared memory; the store counts its bytes off
+// the transaction count of that CTA's mbarrier `rbar` when it lands.
+__device__ __forceinline__ void st_async2(uint32_t addr, const V2& v, uint32_t rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(addr),
+                 "d"(v.v[0]), "d"(v.v[1]), "r"(rbar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx_u32(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t addr, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint32_t addr, uint32_t parity) {
+    if (mbar_try_wait_cluster(addr, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait_cluster(addr, parity)) return true;
+        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
+// Cluster of C = nk / NZ CTAs per field (NZ >= 2, C >= 2); UPT units of two
+// x-adjacent cells of one row per thread, every own plane of each unit.
+template <int NZ, int UPT>
+__global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid_constant__ ClusterArgs a) {
+    constexpr int NPL = NZ + 4;  // planes per buffer: 2 halo, NZ own, 2 halo
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // 2 mbarriers (stage parity)
+    double* buf = reinterpret_cast<double*>(smem_raw + 16);
+    const int ni = a.ni, nj = a.nj, nk = a.nk;
+    const int plane_cells = ni * nj;
+    const uint32_t buf_bytes = (uint32_t)NPL * plane_cells * 8u;
+    const uint32_t base0 = smem_u32(buf);
+    const uint32_t bar0 = smem_u32(bar);
+
+    const uint32_t C = cluster_size();
+    const uint32_t rank = cluster_rank();
+    const int item = blockIdx.x / (int)C;
+    // a converged Parareal slice: the whole cluster leaves before any cluster barrier
+    if (a.item_lo && item + a.item_base < *a.item_lo) return;
+    const uint32_t lower = (rank + C - 1) % C, upper = (rank + 1) % C;
+    const int z0 = (int)rank * NZ;
+    const double* fin = a.in + (long long)item * a.item_stride + a.origin;
+
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        // per stage: this CTA's own arrival with the halo bytes it expects; the
+        // neighbours' stores complete the transaction count
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    const int half = ni / 2;
+    const int units = half * nj;
+    // own cells: unit u -> cells (2*(u % half), u / half) and (+1, same row)
+    int ux[UPT], uy[UPT];
+    bool uv[UPT];
+#pragma unroll
+    for (int j = 0; j < UPT; ++j) {
+        const int u = tid + j * kClusterThreads;
+        uv[j] = u < units;
+        ux[j] = uv[j] ? 2 * (u % half) : 0;
+        uy[j] = uv[j] ? u / half : 0;
+    }
+    // load: own planes into registers and buffer 0; the four halo planes of
+    // buffer 0 from the field's interior (periodic in z)
+    V2 q[UPT][NZ], acc[UPT][NZ];
+#pragma unroll
+    for (int j = 0; j < UPT; ++j)
+#pragma unroll
+        for (int p = 0; p < NPL; ++p) {
+            if (!uv[j]) continue;
+            const int z = (z0 - 2 + p + nk) % nk;
+            const V2 v = ld16<double>(fin + (long long)z * a.plane + (long long)uy[j] * a.px + ux[j]);
+            sts2(base0 + (uint32_t)((p * plane_cells + uy[j] * ni + ux[j]) * 8), v);
+            if (p >= 2 && p < NZ + 2) q[j][p - 2] = v;
+        }
+#pragma unroll
+    for (int j = 0; j < UPT; ++j)
+#pragma unroll
+        for (int o = 0; o < NZ; ++o) acc[j][o] = V2{};
+    __syncthreads();
+    cluster_sync_all();  // every CTA runs and its barriers are initialised before any remote access
+
+    bool bad = false;
+    const int nstage = 4 * a.nsteps;
+    W13<double> w = a.w;
+    // halo bytes per stage: two planes from each z-neighbour
+    const uint32_t halo_bytes = 4u * (uint32_t)plane_cells * 8u;
+    // stage g = 4 * step + ST reads buffer g & 1 and writes buffer (g + 1) & 1
+    auto stage = [&](auto stc, int g) {
+        constexpr int ST = decltype(stc)::value;
+        const uint32_t src = base0 + (uint32_t)(g & 1) * buf_bytes;
+        const uint32_t dst = base0 + (uint32_t)((g + 1) & 1) * buf_bytes;
+        if (g > 0 && !bad) {
+            // halo planes of this stage's input, written by both z-neighbours at the
+            // end of stage g-1 (after one wait has given up, none is tried again:
+            // the kernel runs to its end, reports the timeout and returns)
+            if (!mbar_wait_cluster_bounded(bar0 + 8u * (uint32_t)(g & 1), (uint32_t)(((g - 1) >> 1) & 1))) bad = true;
+        }
+        const bool exchange = g + 1 < nstage;  // the last stage's output goes to global memory only
+        const uint32_t nbar = bar0 + 8u * (uint32_t)((g + 1) & 1);  // completes when stage g+1's halo has landed
+        if (exchange && tid == 0) mbar_arrive_expect_tx_u32(nbar, halo_bytes);
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            if (!uv[j]) continue;
+            const int x = ux[j], y = uy[j];
+            const int xl = (x + ni - 2) % ni, xr = (x + 2) % ni;
+            const int ym1 = (y + nj - 1) % nj, ym2 = (y + nj - 2) % nj, yp1 = (y + 1) % nj, yp2 = (y + 2) % nj;
+            // the unit's column of stage inputs: planes -2 .. NZ+1 (z-window)
+            V2 col[NPL];
+#pragma unroll
+            for (int p = 0; p < NPL; ++p) col[p] = lds2(src + (uint32_t)((p * plane_cells + y * ni + x) * 8));
+#pragma unroll
+            for (int o = 0; o < NZ; ++o) {
+                const int p = o + 2;
+                const uint32_t row = src + (uint32_t)(p * plane_cells * 8);
+                const V2 L = lds2(row + (uint32_t)((y * ni + xl) * 8));
+                const V2 R = lds2(row + (uint32_t)((y * ni + xr) * 8));
+                const V2 Ym1 = lds2(row + (uint32_t)((ym1 * ni + x) * 8));
+                const V2 Ym2 = lds2(row + (uint32_t)((ym2 * ni + x) * 8));
+                const V2 Yp1 = lds2(row + (uint32_t)((yp1 * ni + x) * 8));
+                const V2 Yp2 = lds2(row + (uint32_t)((yp2 * ni + x) * 8));
+                const V2& cen = col[p];
+                const double rowv[6] = {L.v[0], L.v[1], cen.v[0], cen.v[1], R.v[0], R.v[1]};
+                V2 out;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    Nb<double> s;
+                    s.c = rowv[2 + e];
+                    s.xm1 = rowv[1 + e]; s.xp1 = rowv[3 + e];
+                    s.xm2 = rowv[e]; s.xp2 = rowv[4 + e];
+                    s.ym1 = Ym1.v[e]; s.yp1 = Yp1.v[e]; s.ym2 = Ym2.v[e]; s.yp2 = Yp2.v[e];
+                    s.zm1 = col[p - 1].v[e]; s.zp1 = col[p + 1].v[e];
+                    s.zm2 = col[p - 2].v[e]; s.zp2 = col[p + 2].v[e];
+                    const double k = rhs_w13(w, s);
+                    const double qc = q[j][o].v[e];
+                    if constexpr (ST == 0) {
+                        out.v[e] = fma(a.dthalf, k, qc);
+                    } else if constexpr (ST == 1) {
+                        out.v[e] = fma(a.dthalf, k, qc);
+                        acc[j][o].v[e] = fma(a.dt3, k, add_third(cen.v[e], qc, qc));
+                    } else if constexpr (ST == 2) {
+                        out.v[e] = fma(a.dt, k, qc);
+                    } else {
+                        out.v[e] = fma(a.dt6, k, add_third(cen.v[e], qc, acc[j][o].v[e]));
+                    }
+                }
+                if constexpr (ST == 3) q[j][o] = out;
+                const uint32_t cell = (uint32_t)((y * ni + x) * 8);
+                sts2(dst + (uint32_t)(p * plane_cells * 8) + cell, out);
+            }
+        }
+        // own planes of dst written before the next stage reads them, and every
+        // thread of this CTA done reading src: only then may the neighbours
+        // start the next stage, whose halo stores land in the buffer src is
+        __syncthreads();
+        if (exchange) {
+            // the lower neighbour's upper halo planes NZ+2, NZ+3 are our own planes 0, 1;
+            // the upper neighbour's lower halo planes 0, 1 our own planes NZ-2, NZ-1
+#pragma unroll
+            for (int j = 0; j < UPT; ++j) {
+                if (!uv[j]) continue;
+                const uint32_t cell = (uint32_t)((uy[j] * ni + ux[j]) * 8);
+#pragma unroll
+                for (int o = 0; o < NZ; ++o) {
+                    if (o >= 2 && o < NZ - 2) continue;
+                    const V2 v = lds2(dst + (uint32_t)((o + 2) * plane_cells * 8) + cell);
+                    if (o < 2)
+                        st_async2(map_rank(dst + (uint32_t)((NZ + 2 + o) * plane_cells * 8) + cell, lower), v,
+                                  map_rank(nbar, lower));
+                    if (o >= NZ - 2)
+                        st_async2(map_rank(dst + (uint32_t)((o - (NZ - 2)) * plane_cells * 8) + cell, upper), v,
+                                  map_rank(nbar, upper));
+                }
+            }
+        }
+    };
+    for (int i = 0; i < a.nsteps; ++i) {
+        if (a.wtab) w = a.wtab[i];
+        stage(std::integral_constant<int, 0>{}, 4 * i);
+        stage(std::integral_constant<int, 1>{}, 4 * i + 1);
+        stage(std::integral_constant<int, 2>{}, 4 * i + 2);
+        stage(std::integral_constant<int, 3>{}, 4 * i + 3);
+    }
+    // result (the last stage's q') to global memory, interior only (the host
+    // fills the periodic images)
+    double* fout = a.out + (long long)item * a.item_stride + a.origin;
+#pragma unroll
+    for (int j = 0; j < UPT; ++j)
+#pragma unroll
+        for (int o = 0; o < NZ; ++o)
+            if (uv[j]) gst16<double>(a.sb, fout + (long long)(z0 + o) * a.plane + (long long)uy[j] * a.px + ux[j], q[j][o]);
+    if (__syncthreads_or(bad) && tid == 0) atomicExch(a.err, DEV_WAIT_TIMEOUT);
+    cluster_sync_all();  // no CTA leaves while a neighbour may still address its shared memory
+}
+
+template <int NZ, int UPT>
+size_t cluster_smem(const Geo& g) {
+    return 16 + (size_t)2 * (NZ + 4) * g.ni * g.nj * 8;
+}
+
+template <int NZ, int UPT>
+cudaError_t set_attr_cluster(const Geo* g) {
+    auto k = k_rk4_cluster<NZ, UPT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmemMax);
+    (void)g;
+    return e;
+}
+
+// Planes per CTA for a grid and batch: NZ in {2, 3, 4} with a cluster of at
+// most 16 CTAs whose buffers fit -- the smallest (the most CTAs per field: a
+// single field is bound by the latency of each stage) while the batch's CTAs
+// fit on the SMs at once, else the largest (fewer CTAs per field, more fields
+// at a time); 0 when the grid is not supported.
+int cluster_nz(const Geo& g, int items = 1) {
+    if (g.es != 8 || g.ni % 2 != 0 || g.ni < 4 || g.nj < 4 || g.nk < 4) return 0;
+    if ((long long)(g.ni / 2) * g.nj > 2LL * kClusterThreads) return 0;
+    int first = 0, last = 0;
+    for (int nz : {2, 3, 4}) {
+        if (g.nk % nz != 0) continue;
+        const int c = g.nk / nz;
+        if (c < 2 || c > 16) continue;
+        if (16 + (size_t)2 * (nz + 4) * g.ni * g.nj * 8 > (size_t)kClusterSmemMax) continue;
+        if (!first) first = nz;
+        last = nz;
+    }
+    if (!first) return 0;
+    return (long long)items * (g.nk / first) <= 148 ? first : last;
+}
+
+template <int NZ, int UPT>
+cudaError_t launch_one(const Geo& g, const ClusterArgs& a, int items, cudaStream_t s) {
+    const int C = g.nk / NZ;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(C * items));
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = cluster_smem<NZ, UPT>(g);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_rk4_cluster<NZ, UPT>, a);
+}
+
+}  // namespace
+
+bool cluster_supported(const Geo& g) { return cluster_nz(g) != 0; }
+
+cudaError_t prepare_cluster() {
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    chk(set_attr_cluster<2, 1>(nullptr)); chk(set_attr_cluster<2, 2>(nullptr));
+    chk(set_attr_cluster<3, 1>(nullptr)); chk(set_attr_cluster<3, 2>(nullptr));
+    chk(set_attr_cluster<4, 1>(nullptr)); chk(set_attr_cluster<4, 2>(nullptr));
+    return e;
+}
+
+cudaError_t launch_rk4_cluster(const Geo& g, const ClusterLaunch& L, cudaStream_t s, int* err) {
+    const int nz = cluster_nz(g, L.items);
+    if (!nz || L.nsteps < 1 || L.items < 1) return cudaErrorInvalidValue;
+    ClusterArgs a;
+    a.in = static_cast<const double*>(L.in);
+    a.out = static_cast<double*>(L.out);
+    a.item_stride = g.total;
+    a.origin = g.origin;
+    a.px = g.px;
+    a.plane = g.plane;
+    a.ni = g.ni; a.nj = g.nj; a.nk = g.nk;
+    a.nsteps = L.nsteps;
+    a.wtab = static_cast<const W13<double>*>(L.wtab);
+    fill_w13(a.w, L.coef, L.nu);
+    a.dthalf = L.dt * .5;
+    a.dt = L.dt;
+    a.dt3 = L.dt / 3.;
+    a.dt6 = L.dt / 6.;
+    a.item_lo = L.item_lo;
+    a.item_base = L.item_base;
+    a.err = err;
+    a.sb = out_bounds(L.out, g, L.items);
+    const bool two = (long long)(g.ni / 2) * g.nj > kClusterThreads;
+    add_launches(1);
+    switch (nz * 2 + (two ? 1 : 0)) {
+        case 4: return launch_one<2, 1>(g, a, L.items, s);
+        case 5: return launch_one<2, 2>(g, a, L.items, s);
+        case 6: return launch_one<3, 1>(g, a, L.items, s);
+        case 7: return launch_one<3, 2>(g, a, L.items, s);
+        case 8: return launch_one<4, 1>(g, a, L.items, s);
+        default: return launch_one<4, 2>(g, a, L.items, s);
+    }
+}
+
+void fill_cluster_weights(void* w13, const Coef& c, double nu) { fill_w13(*static_cast<W13<double>*>(w13), c, nu); }
+
+size_t cluster_weights_bytes() { return sizeof(W13<double>); }
+
+}  // namespace sp

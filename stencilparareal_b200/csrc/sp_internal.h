@@ -43,6 +43,7 @@ struct Tune {
     Shape op[kNumOps];
     Shape pair[2] = {Shape{8, 0, 1}, Shape{8, 0, 1}};  // fused stage pairs 1+2 and 3+4 (ty 8 or 16)
     int fused = 0;    // 1: FP64 RK4 steps run as the two fused pairs
+    int cluster = 0;  // 1: FP64 RK4 propagations of small fields run cluster-resident (sp_cluster.cu)
     void set_all(const Shape& s) {
         for (auto& o : op) o = s;
     }
@@ -87,6 +88,30 @@ struct StageLaunch {
     double dnu = 1;                  // d nu / d nu0
     int adj_first = 0;               // 1: lam_acc = lam + ybar (first adjoint stage of a step)
 };
+
+// Many FP64 RK4 steps of small fields in one launch, each field held in the
+// distributed shared memory of one thread-block cluster (sp_cluster.cu).  Reads
+// the interiors of `items` fields at `in`, writes the interiors of the results
+// at `out` (in == out allowed; the periodic images of `out` are left to the
+// caller).  Step i uses the weights of `nu`, or wtab[i] (cluster_weights_bytes()
+// each, device memory) when wtab is set.
+struct ClusterLaunch {
+    const void* in = nullptr;
+    void* out = nullptr;
+    int items = 1;
+    int nsteps = 0;
+    double dt = 0, nu = 0;
+    Coef coef;
+    const void* wtab = nullptr;
+    const int* item_lo = nullptr;    // as in StageLaunch
+    int item_base = 0;
+};
+bool cluster_supported(const Geo& g);  // FP64, even ni, small planes, nk = C * {2,3,4} with 2 <= C <= 16
+cudaError_t prepare_cluster();
+cudaError_t launch_rk4_cluster(const Geo& g, const ClusterLaunch& L, cudaStream_t s, int* err);
+size_t cluster_weights_bytes();
+void fill_cluster_weights(void* w13, const Coef& c, double nu);  // one entry of wtab (host memory)
+constexpr int kClusterSmemMax = 227 * 1024;
 
 // Launches one stage kernel; counts the launch.  err: device error word.
 cudaError_t launch_stage(const Geo& g, const StageLaunch& L, const Tune& t, cudaStream_t s, int* err);

@@ -767,6 +767,7 @@ cudaError_t prepare_kernels() {
     chk(set_attr_op<float, OP_RK_S3>()); chk(set_attr_op<float, OP_RK_S4>());
     chk(set_attr_op<float, OP_EULER>());
     chk(prepare_pairs());
+    chk(prepare_cluster());
     return e;
 }
 

@@ -122,6 +122,7 @@ struct sp_convection {
     DevBuf red;         // reduction scratch (8 doubles)
     DevBuf dense;       // staging for the host-buffer entry point
     DevBuf adj_ckpt, adj_seg, adj_work, adj_par;  // adjoint workspace, kept between calls
+    DevBuf ctab;        // per-step stencil weights of the cluster-resident path (nu(t) varies)
     std::map<std::tuple<int, int>, Tune> tunes;  // (prec, items) -> tune
     std::map<std::tuple<int, const void*, double, double, int>, GraphEntry> graphs;
     cudaStream_t stream() const { return user ? user : own; }
@@ -369,7 +370,31 @@ int do_prop(sp_convection* h, int prec, bool rk, const void* in, void* out, doub
     // Periodicity on the input, in place, as before the reference's first stencil.
     SP_CUDA(launch_periodicity(g, const_cast<void*>(in), 1, s));
     const bool const_nu = h->P.nufreq == 0.;
-    if (rk && t.fused && prec == 0 && pair_supported(h->g4)) {
+    if (rk && t.cluster && prec == 0 && cluster_supported(g) && (const_nu || !capturing(s))) {
+        // small field: every step in one launch, the field held in a cluster's
+        // shared memory (sp_cluster.cu); then the periodic images of `out`
+        ClusterLaunch L;
+        L.in = in;
+        L.out = out;
+        L.nsteps = n;
+        L.dt = dt;
+        L.coef = h->coef;
+        L.nu = computenu(h->P.nu0, h->P.nufreq, tStart);
+        if (!const_nu) {
+            // nu(tStart + i dt) per step (Convection.cpp:296-302), as weights
+            const size_t wb = cluster_weights_bytes();
+            std::vector<unsigned char> tab((size_t)n * wb);
+            for (int i = 0; i < n; ++i)
+                fill_cluster_weights(tab.data() + (size_t)i * wb, h->coef,
+                                     computenu(h->P.nu0, h->P.nufreq, i == 0 ? tStart : tStart + i * dt));
+            if (h->ctab.alloc(tab.size()) != cudaSuccess) return fail(SP_ERR_NOMEM, "weight table");
+            SP_CUDA(cudaMemcpyAsync(h->ctab.p, tab.data(), tab.size(), cudaMemcpyHostToDevice, s));
+            SP_CUDA(cudaStreamSynchronize(s));  // the host table goes out of scope
+            L.wtab = h->ctab.p;
+        }
+        SP_CUDA(launch_rk4_cluster(g, L, s, err));
+        SP_CUDA(launch_periodicity(g, out, 1, s));
+    } else if (rk && t.fused && prec == 0 && pair_supported(h->g4)) {
         // fused stage pairs: widen the input once, alternate the step-start
         // field between wbuf(0) and wbuf(1), write the last step to `out`
         if ((rc = h->ensure_wide(1))) return rc;
@@ -515,7 +540,18 @@ int sp_convection_synchronize(sp_convection* h) {
 
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
-    if (kind < 0 || kind > 2) return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA) or 2 (fused pairs)");
+    if (kind < 0 || kind > 3)
+        return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA), 2 (fused pairs) or 3 (cluster-resident)");
+    if (kind == 3) {
+        if (precision != SP_F64 || !cluster_supported(h->g[0]))
+            return fail(SP_ERR_INVALID, "the cluster-resident path needs FP64, an even ni, small planes and nk = C x "
+                                        "{2,3,4} with 2 <= C <= 16");
+        Tune t = h->tune(precision, batch);
+        t.cluster = 1;
+        h->tunes[{precision, batch}] = t;
+        h->drop_graphs();
+        return SP_OK;
+    }
     if (zchunk < (kind == 2 ? 0 : 1))
         return fail(SP_ERR_INVALID, "zchunk must be >= 1 (>= 0 for fused pairs: planes per CTA, 0 = automatic)");
     if (kind == 2) {
@@ -546,7 +582,8 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
 }
 
 // op 0..8: single-stage kernels (tma: 0 direct, 1 TMA); op 9, 10: fused pairs
-// 1+2 and 3+4 (tma: 2 when RK4 steps run fused, else 0).
+// 1+2 and 3+4 (tma: 2 when RK4 steps run fused, else 0); op 11: the
+// cluster-resident path (tma: 3 when FP64 RK4 propagations use it, else 0).
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* tma) {
     if (!h) return fail(SP_ERR_INVALID, "null handle");
     const Tune tn = h->tune(precision, batch);
@@ -555,6 +592,9 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
     if (op == kNumOps || op == kNumOps + 1) {
         t = tn.pair[op - kNumOps];
         kind = tn.fused ? 2 : 0;
+    } else if (op == kNumOps + 2) {
+        t = Shape{0, 0, 0};
+        kind = tn.cluster ? 3 : 0;
     } else {
         t = tn.op[op < 0 || op >= kNumOps ? OP_RK_S2 : op];
         kind = t.tma;
@@ -958,6 +998,53 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
             }
         }
     }
+    // small fields: the cluster-resident path against the best of the above,
+    // timed as it is used (a DoRK4 of a graph chunk of steps for one field; four
+    // batched steps for a batch)
+    best.cluster = 0;
+    if (precision == SP_F64 && cluster_supported(g)) {
+        int* err = h->err.as<int>();
+        float path_ms[2] = {1e30f, 1e30f};
+        SP_CUDA(cudaMemsetAsync(p, 0, 5 * fb, s));
+        for (int c = 0; c < 2 && rc == SP_OK; ++c) {
+            Tune tt = best;
+            tt.cluster = c;
+            h->tunes[{precision, batch}] = tt;
+            h->drop_graphs();
+            auto run = [&]() -> int {
+                if (batch == 1) return do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);
+                const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
+                cudaError_t x = cudaSuccess;
+                if (c) {
+                    ClusterLaunch L;
+                    L.in = p; L.out = p; L.items = batch; L.nsteps = 4; L.dt = 1e-9; L.nu = nu; L.coef = h->coef;
+                    x = launch_rk4_cluster(g, L, s, err);
+                } else {
+                    for (int i = 0; i < 4 && x == cudaSuccess; ++i)
+                        x = enqueue_rk4_step(g, precision, h->coef, 1e-9, NuSrc{nu, nullptr}, p, p, p + fb, p + 2 * fb,
+                                             p + 3 * fb, batch, nullptr, 0, tt, s, err);
+                }
+                return x == cudaSuccess ? SP_OK : fail(SP_ERR_CUDA, "tuning: %s", cudaGetErrorString(x));
+            };
+            rc = run();  // captures the graphs / warms up
+            for (int r = 0; r < 3 && rc == SP_OK; ++r) {
+                cudaEventRecord(e0, s);
+                rc = run();
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float m = 0;
+                cudaEventElapsedTime(&m, e0, e1);
+                path_ms[c] = std::min(path_ms[c], m);
+            }
+        }
+        if (rc != SP_OK) {
+            // the cluster launch can be refused (cluster shape not schedulable): keep the other path
+            cudaGetLastError();
+            rc = SP_OK;
+            path_ms[1] = 1e30f;
+        }
+        best.cluster = path_ms[1] < path_ms[0] ? 1 : 0;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     SP_CUDA(cudaStreamSynchronize(s));
@@ -1175,15 +1262,21 @@ int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0,
 // parts: 1 = F sweep, 2 = G sweep, 3 = both.  zero_min: in the increment form the
 // G sweep zeroes the increment of its first iterating slice unless that is a slice
 // below zero_min (a window's slice 0 gets its increment from the previous window).
+// The F sweep's path: every step of all slices in one cluster-resident launch
+// (small fields), fused stage pairs, or the four stage kernels per step.
+bool cluster_sweep(const sp_parareal* pr) {
+    sp_convection* h = pr->prop;
+    return h->P.nufreq == 0. && h->tune(0, pr->P).cluster && cluster_supported(pr->g64);
+}
 bool fused_sweep(const sp_parareal* pr) {
     sp_convection* h = pr->prop;
-    return h->P.nufreq == 0. && h->tune(0, pr->P).fused && pair_supported(h->g4);
+    return !cluster_sweep(pr) && h->P.nufreq == 0. && h->tune(0, pr->P).fused && pair_supported(h->g4);
 }
 
 // Allocates the fine-sweep scratch of the path the tune selects; must run
 // before a capture of the iteration.
 int prepare_iteration(sp_parareal* pr, int parts) {
-    if (!(parts & 1)) return SP_OK;
+    if (!(parts & 1) || cluster_sweep(pr)) return SP_OK;
     const int P = pr->P;
     const Geo& g = pr->g64;
     const Geo& g4 = pr->prop->g4;
@@ -1218,6 +1311,21 @@ int emit_iteration(sp_parareal* pr, cudaStream_t s, bool events, int parts, int 
     double* acc = yb + fstride;
     int rc = SP_OK;
     cudaError_t e = events ? cudaEventRecordWithFlags(pr->ev[0], s, cudaEventRecordExternal) : cudaSuccess;
+    const bool cluster = cluster_sweep(pr);
+    if (cluster && (parts & 1) && e == cudaSuccess) {
+        // every fine step of every iterating slice in one launch, each slice in one cluster
+        ClusterLaunch L;
+        L.in = pr->u(0);
+        L.out = pr->f(0);
+        L.items = P;
+        L.nsteps = pr->tsF;
+        L.dt = pr->dtF;
+        L.nu = h->P.nu0;
+        L.coef = h->coef;
+        L.item_lo = pr->itemlo();
+        e = launch_rk4_cluster(g, L, s, err);
+        if (e == cudaSuccess) e = launch_periodicity(g, pr->f(0), P, s);
+    }
     if (fused && (parts & 1)) {
         // widen the slice inputs once, alternate step start / accumulator
         // between W0 and W1, write the last step into the fine results
@@ -1242,7 +1350,7 @@ int emit_iteration(sp_parareal* pr, cudaStream_t s, bool events, int parts, int 
             if (e == cudaSuccess) e = launch_pair(g4, last ? g : g4, L, tf.pair[1], s, err);
         }
     }
-    for (int i = 0; i < pr->tsF && e == cudaSuccess && (parts & 1) && !fused; ++i) {
+    for (int i = 0; i < pr->tsF && e == cudaSuccess && (parts & 1) && !fused && !cluster; ++i) {
         NuSrc nu;
         if (const_nu) nu.nu = h->P.nu0;
         else nu.items = pr->nutab.as<double>() + (size_t)i * P;

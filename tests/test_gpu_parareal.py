@@ -232,13 +232,18 @@ def test_one_launch_loop_equals_host_loop(sp, tol_kind, tol):
                           tol_kind=tol_kind)
         par.set_host_loop(host)
         rep = par.DoParallel(reference=fref)
+        first = conv.download(fsol)
         rep2 = par.DoParallel(reference=fref)  # a second run of the same graph
-        assert rep2["iterations"] == rep["iterations"] and rep2["defect"] == rep["defect"]
-        outs.append((conv.download(fsol), rep))
+        assert np.array_equal(conv.download(fsol), first)
+        assert rep2["iterations"] == rep["iterations"]
+        outs.append((first, rep))
     (a, ra), (b, rb) = outs
     assert np.array_equal(a, b)
     assert ra["iterations"] == rb["iterations"]
-    assert ra["defect"] == rb["defect"] and ra["err_l2"] == rb["err_l2"] and ra["err_max"] == rb["err_max"]
+    # the defect and error sums are accumulated with atomics across CTAs, so
+    # their last bits depend on the order of the additions
+    for key in ("defect", "err_l2", "err_max"):
+        assert np.allclose(ra[key], rb[key], rtol=1e-12, atol=0), key
     assert ra["fine_cell_updates"] == rb["fine_cell_updates"]
     if tol_kind == "none":
         assert ra["iterations"] == 5
@@ -272,6 +277,8 @@ def test_batch_one_launch_loop_equals_host_loop(sp):
     for x, y in zip(fa, fb):
         assert np.array_equal(x, y)
     for x, y in zip(ra, rb):
-        assert x["iterations"] == y["iterations"] and x["defect"] == y["defect"] and x["err_l2"] == y["err_l2"]
+        assert x["iterations"] == y["iterations"]
+        assert np.allclose(x["defect"], y["defect"], rtol=1e-12, atol=0)
+        assert np.allclose(x["err_l2"], y["err_l2"], rtol=1e-12, atol=0)
         assert x["fine_cell_updates"] == y["fine_cell_updates"]
     assert ra[2]["iterations"] == 3  # no tolerance: exact after P = 3 iterations
