@@ -320,8 +320,11 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
         conv = sp.Convection(n, n, n, 1.0 / n, nu, 0.0, *c, device=device)
         if n not in tunes:
             a64 = conv.autotune(sp.SP_F64, 16)
-            # fused stage pairs when the tuner preferred them, else the stage kernels' shape
-            tunes[n] = (a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"], conv.autotune(sp.SP_F32, 1)["S2"])
+            # the cluster-resident path or the fused stage pairs when the tuner
+            # preferred them, else the stage kernels' shape
+            t64 = (a64["cluster"] if a64["cluster"]["kind"] == 3 else
+                   a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"])
+            tunes[n] = (t64, conv.autotune(sp.SP_F32, 1)["S2"])
         t64, t32 = tunes[n]
         conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
         conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
@@ -475,7 +478,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", default="auto", help="'auto' or ty,zchunk,kind for the stage kernels")
     ap.add_argument("--profile", action="store_true",
-                    help="profiling run: one 256^3 DoRK4 of 2 steps with the given --tune, no timing")
+                    help="profiling run: one DoRK4 of --profile-steps steps on the 256^3 workload (or a "
+                         "--profile-grid cube with the Gaussian+noise field) with the given --tune, no timing")
+    ap.add_argument("--profile-grid", type=int, default=N_FINE)
+    ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--no-pipeline", action="store_true", help="N>1: skip the Parareal slice pipeline")
     ap.add_argument("--pipeline-only", action="store_true",
                     help="N>1: run only the Parareal slice pipeline (prints its JSON object)")
@@ -510,7 +516,7 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
             return 0
-    n = N_FINE
+    n = args.profile_grid if args.profile else N_FINE
     conv = sp.Convection(n, n, n, 1.0 / n, NU, 0.0, C[0], C[1], C[2], device=device)
     if args.tune == "auto" and not args.profile:
         tune = conv.autotune(sp.SP_F64, 1)
@@ -518,13 +524,20 @@ def main():
         ty, zc, kind = (int(x) for x in (args.tune if args.tune != "auto" else "4,8,1").split(","))
         conv.set_tune(sp.SP_F64, 1, ty, zc, kind)
         tune = conv.tuned_configs(sp.SP_F64, 1)
-    q0 = fourier_ic(n)
+    if n == N_FINE:
+        q0 = fourier_ic(n)
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from ics import gaussian_noise
+        q0 = gaussian_noise(n, seed=0)
     fin, fout = conv.field(), conv.field()
     conv.upload(fin, q0)
     if args.profile:
-        conv.DoRK4(fin, fout, 0.0, DT, 2)
+        conv.DoRK4(fin, fout, 0.0, DT, args.profile_steps)
         conv.synchronize()
-        print(json.dumps({"profile": WORKLOAD.replace(f"x {STEPS_PER_RUN} steps", "x 2 steps"), "tune": tune}))
+        what = (WORKLOAD.replace(f"x {STEPS_PER_RUN} steps", f"x {args.profile_steps} steps") if n == N_FINE
+                else f"fine RK4 FP64 {n}^3 x {args.profile_steps} steps, Gaussian+noise IC seed 0")
+        print(json.dumps({"profile": what, "tune": tune}))
         return 0
     stream = conv.stream
 

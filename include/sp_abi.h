@@ -276,9 +276,10 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
  * stage kernel gets the fastest of its candidate launch shapes, and FP64 RK4
  * steps run as fused pairs when those are more than 2 % faster than the four
  * stages: for batch 1 as timed through sp_do_rk4 (a graph chunk of 50 steps on
- * scratch fields), for larger batches over four consecutive batched steps.
- * Small FP64 fields then take the cluster-resident path (kind 3 of
- * sp_set_tune) when it is faster, timed the same way. */
+ * scratch fields), for larger batches over four consecutive batched steps, each
+ * path timed after 0.4 s of running back to back (at the clocks it sustains
+ * under the GPU's power cap).  Small FP64 fields then take the
+ * cluster-resident path (kind 3 of sp_set_tune) when it is faster. */
 int sp_autotune(sp_convection* h, int precision, int batch);
 /* Test of the error path of the bounded in-kernel waits: runs one kernel whose
  * wait can never complete and gives up after limit_ms (<= 2000); returns
