@@ -149,7 +149,15 @@ __device__ __forceinline__ void cell_op(const KArgs<T>& a, T nl, const Nb<T>& s,
         const T dqy = diff_mode(a.m1, s.c, s.ym1, s.yp1);
         const T dqz = diff_mode(a.m2, s.c, s.zm1, s.zp1);
         const T adv = fmaT(a.u0, dqx, fmaT(a.u1, dqy, a.u2 * dqz));
-        const T lap = ((s.xm1 + s.xp1) + (s.ym1 + s.yp1) + (s.zm1 + s.zp1)) - T(6) * s.c;
+        T lap;
+        if constexpr (sizeof(T) == 4) {
+            // FP32: the sum of the neighbours' differences from the centre (exact
+            // and small), not the cancelling S1 - 6q (see rhs_w13)
+            const T c = s.c;
+            lap = ((s.xm1 - c) + (s.xp1 - c)) + ((s.ym1 - c) + (s.yp1 - c)) + ((s.zm1 - c) + (s.zp1 - c));
+        } else {
+            lap = ((s.xm1 + s.xp1) + (s.ym1 + s.yp1) + (s.zm1 + s.zp1)) - T(6) * s.c;
+        }
         const T k = fmaT(nl, lap, adv);
         oy = fmaT(a.c_y, k, s.c);
         (void)p0; (void)p1; (void)p2; (void)oa; (void)g; (void)live;
@@ -157,9 +165,19 @@ __device__ __forceinline__ void cell_op(const KArgs<T>& a, T nl, const Nb<T>& s,
         const T ax = fmaT(T(8), s.xm1 - s.xp1, s.xp2 - s.xm2);
         const T ay = fmaT(T(8), s.ym1 - s.yp1, s.yp2 - s.ym2);
         const T az = fmaT(T(8), s.zm1 - s.zp1, s.zp2 - s.zm2);
-        const T S1 = (s.xm1 + s.xp1) + (s.ym1 + s.yp1) + (s.zm1 + s.zp1);
-        const T S2 = (s.xm2 + s.xp2) + (s.ym2 + s.yp2) + (s.zm2 + s.zp2);
-        const T lap = fmaT(T(-90), s.c, fmaT(T(16), S1, -S2));
+        T lap;
+        if constexpr (sizeof(T) == 4) {
+            // FP32: 16 D1 - D2 with D1, D2 the neighbours' differences from the
+            // centre (equal to -90 q + 16 S1 - S2; see rhs_w13)
+            const T c = s.c;
+            const T D1 = ((s.xm1 - c) + (s.xp1 - c)) + ((s.ym1 - c) + (s.yp1 - c)) + ((s.zm1 - c) + (s.zp1 - c));
+            const T D2 = ((s.xm2 - c) + (s.xp2 - c)) + ((s.ym2 - c) + (s.yp2 - c)) + ((s.zm2 - c) + (s.zp2 - c));
+            lap = fmaT(T(16), D1, -D2);
+        } else {
+            const T S1 = (s.xm1 + s.xp1) + (s.ym1 + s.yp1) + (s.zm1 + s.zp1);
+            const T S2 = (s.xm2 + s.xp2) + (s.ym2 + s.yp2) + (s.zm2 + s.zp2);
+            lap = fmaT(T(-90), s.c, fmaT(T(16), S1, -S2));
+        }
         const T adv = fmaT(a.ca0, ax, fmaT(a.ca1, ay, a.ca2 * az));
         if constexpr (!OpTraits<OP>::adjoint) {
             const T k = fmaT(nl, lap, adv);

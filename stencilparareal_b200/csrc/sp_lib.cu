@@ -839,6 +839,32 @@ extern "C" int sp_kernel_times(sp_convection* h, const double* field, double dt,
     return sp_convection_synchronize(h);
 }
 
+namespace {
+// Tuning data: the paths are timed on fields of varying values at a stable
+// step, as they run in practice.  On all-zero fields at a vanishing step the
+// kernels draw far less power and never reach the GPU's power cap, which
+// decides between them on real data.
+template <typename T>
+__global__ void k_fill_wave(T* p, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = (T)(sin(1e-3 * (double)i) + 0.25 * sin(0.37 * (double)i));
+}
+cudaError_t fill_wave(void* p, size_t bytes, int es, cudaStream_t s) {
+    const long long n = (long long)(bytes / es);
+    if (es == 8) k_fill_wave<double><<<1184, 256, 0, s>>>(static_cast<double*>(p), n);
+    else k_fill_wave<float><<<1184, 256, 0, s>>>(static_cast<float*>(p), n);
+    return cudaGetLastError();
+}
+// A tenth of RK4's stability bound for this grid's velocity and diffusivity.
+double tune_dt(const sp_convection* h) {
+    const double dx = h->P.dx;
+    const double adv = (std::fabs(h->P.cx) + std::fabs(h->P.cy) + std::fabs(h->P.cz)) * 1.5 / dx;
+    const double dif = 1.5 * std::fabs(h->P.nu0) * 3. * 16. / 12. / (dx * dx);  // nu(t) <= 1.5 nu0
+    const double lam = adv + dif;
+    return lam > 0 ? 0.1 * 2.78 / lam : 1e-9;
+}
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // Autotuner: for every stage kernel (RK4 S1..S4, Euler) times each candidate
 // launch shape (kernel kind x tile rows x z-chunk) on scratch fields and keeps
@@ -855,6 +881,8 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     const size_t fb = (size_t)batch * g.total * g.es;
     if (buf.alloc(5 * fb) != cudaSuccess) return fail(SP_ERR_NOMEM, "tuning buffers");
     char* p = buf.as<char>();
+    SP_CUDA(fill_wave(p, 5 * fb, g.es, s));
+    const double dtt = tune_dt(h);
     cudaEvent_t e0, e1;
     SP_CUDA(cudaEventCreate(&e0));
     SP_CUDA(cudaEventCreate(&e1));
@@ -943,19 +971,19 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 // steps), where consecutive kernels overlap through programmatic
                 // dependent launch and four stage kernels overlap more than two
                 // pairs, so that the sums of isolated kernel times mislead.
-                SP_CUDA(cudaMemsetAsync(p, 0, 2 * fb, s));
+                SP_CUDA(fill_wave(p, 2 * fb, g.es, s));
                 float path_ms[2] = {1e30f, 1e30f};
                 for (int f = 0; f < 2 && rc == SP_OK; ++f) {
                     Tune tt = best;
                     tt.fused = f;
                     h->tunes[{precision, batch}] = tt;
                     h->drop_graphs();
-                    rc = do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);  // captures the graph
+                    rc = do_prop(h, precision, true, p, p + fb, 0.0, dtt, kChunk + 1);  // captures the graph
                     if (rc == SP_OK)  // at the clocks the path sustains
-                        rc = sustain(s, [&]() { return do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1); });
+                        rc = sustain(s, [&]() { return do_prop(h, precision, true, p, p + fb, 0.0, dtt, kChunk + 1); });
                     for (int r = 0; r < 3 && rc == SP_OK; ++r) {
                         cudaEventRecord(e0, s);
-                        rc = do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);
+                        rc = do_prop(h, precision, true, p, p + fb, 0.0, dtt, kChunk + 1);
                         cudaEventRecord(e1, s);
                         cudaEventSynchronize(e1);
                         float m = 0;
@@ -973,8 +1001,8 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
             } else {
                 // Batches (the Parareal F sweep): four consecutive batched steps of
                 // each path as the sweep launches them, after one untimed step.
-                SP_CUDA(cudaMemsetAsync(p, 0, 4 * fb, s));
-                SP_CUDA(cudaMemsetAsync(w, 0, 3 * wb, s));
+                SP_CUDA(fill_wave(p, 4 * fb, g.es, s));
+                SP_CUDA(fill_wave(w, 3 * wb, g4.es, s));
                 const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
                 int* err = h->err.as<int>();
                 Tune ts = best;
@@ -982,7 +1010,7 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 auto stage_steps = [&](int k) {
                     cudaError_t x = cudaSuccess;
                     for (int i = 0; i < k && x == cudaSuccess; ++i)
-                        x = enqueue_rk4_step(g, precision, h->coef, 1e-9, NuSrc{nu, nullptr}, p, p, p + fb,
+                        x = enqueue_rk4_step(g, precision, h->coef, dtt, NuSrc{nu, nullptr}, p, p, p + fb,
                                              p + 2 * fb, p + 3 * fb, batch, nullptr, 0, ts, s, err);
                     return x;
                 };
@@ -991,7 +1019,7 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                     for (int i = 0; i < k && x == cudaSuccess; ++i) {
                         char* Q = w + (size_t)(i % 2) * wb;
                         char* A = w + (size_t)((i + 1) % 2) * wb;
-                        x = enqueue_pair_step(h, best, 1e-9, nu, Q, A, w + 2 * wb, A, h->g4, batch, nullptr, 0, s,
+                        x = enqueue_pair_step(h, best, dtt, nu, Q, A, w + 2 * wb, A, h->g4, batch, nullptr, 0, s,
                                               err);
                     }
                     return x;
@@ -1033,23 +1061,23 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
     if (precision == SP_F64 && cluster_supported(g)) {
         int* err = h->err.as<int>();
         float path_ms[2] = {1e30f, 1e30f};
-        SP_CUDA(cudaMemsetAsync(p, 0, 5 * fb, s));
+        SP_CUDA(fill_wave(p, 5 * fb, g.es, s));
         for (int c = 0; c < 2 && rc == SP_OK; ++c) {
             Tune tt = best;
             tt.cluster = c;
             h->tunes[{precision, batch}] = tt;
             h->drop_graphs();
             auto run = [&]() -> int {
-                if (batch == 1) return do_prop(h, precision, true, p, p + fb, 0.0, 1e-9, kChunk + 1);
+                if (batch == 1) return do_prop(h, precision, true, p, p + fb, 0.0, dtt, kChunk + 1);
                 const double nu = computenu(h->P.nu0, h->P.nufreq, 0.0);
                 cudaError_t x = cudaSuccess;
                 if (c) {
                     ClusterLaunch L;
-                    L.in = p; L.out = p; L.items = batch; L.nsteps = 4; L.dt = 1e-9; L.nu = nu; L.coef = h->coef;
+                    L.in = p; L.out = p; L.items = batch; L.nsteps = 4; L.dt = dtt; L.nu = nu; L.coef = h->coef;
                     x = launch_rk4_cluster(g, L, s, err);
                 } else {
                     for (int i = 0; i < 4 && x == cudaSuccess; ++i)
-                        x = enqueue_rk4_step(g, precision, h->coef, 1e-9, NuSrc{nu, nullptr}, p, p, p + fb, p + 2 * fb,
+                        x = enqueue_rk4_step(g, precision, h->coef, dtt, NuSrc{nu, nullptr}, p, p, p + fb, p + 2 * fb,
                                              p + 3 * fb, batch, nullptr, 0, tt, s, err);
                 }
                 return x == cudaSuccess ? SP_OK : fail(SP_ERR_CUDA, "tuning: %s", cudaGetErrorString(x));

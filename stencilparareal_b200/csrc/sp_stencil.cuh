@@ -40,12 +40,27 @@ struct Nb {
     T c, xm1, xp1, xm2, xp2, ym1, yp1, ym2, yp2, zm1, zp1, zm2, zp2;
 };
 
+// FP64: the 13 products.  FP32 (the coarse propagator): the weights sum to
+// zero (the stencils are consistent), so R = sum over the 12 neighbours of
+// w_o (q_o - q_c) exactly; the differences of nearby values are exact in FP32
+// and small, where the 13 products of O(1) values with weights up to
+// 90 nu/(12 dx^2) would cancel to a result ~1e-4 as large as themselves, and
+// the FP32-rounded weights would no longer sum to zero (a drift of every
+// field, ~7e-7 per 7 coarse steps at 128^3).
 template <typename T>
 __device__ __forceinline__ T rhs_w13(const W13<T>& w, const Nb<T>& s) {
-    const T sx = fmaT(w.m2[0], s.xm2, fmaT(w.m1[0], s.xm1, fmaT(w.p1[0], s.xp1, w.p2[0] * s.xp2)));
-    const T sy = fmaT(w.m2[1], s.ym2, fmaT(w.m1[1], s.ym1, fmaT(w.p1[1], s.yp1, w.p2[1] * s.yp2)));
-    const T sz = fmaT(w.m2[2], s.zm2, fmaT(w.m1[2], s.zm1, fmaT(w.p1[2], s.zp1, w.p2[2] * s.zp2)));
-    return fmaT(w.c, s.c, (sx + sy) + sz);
+    if constexpr (sizeof(T) == 4) {
+        const T c = s.c;
+        const T sx = fmaT(w.m2[0], s.xm2 - c, fmaT(w.m1[0], s.xm1 - c, fmaT(w.p1[0], s.xp1 - c, w.p2[0] * (s.xp2 - c))));
+        const T sy = fmaT(w.m2[1], s.ym2 - c, fmaT(w.m1[1], s.ym1 - c, fmaT(w.p1[1], s.yp1 - c, w.p2[1] * (s.yp2 - c))));
+        const T sz = fmaT(w.m2[2], s.zm2 - c, fmaT(w.m1[2], s.zm1 - c, fmaT(w.p1[2], s.zp1 - c, w.p2[2] * (s.zp2 - c))));
+        return (sx + sy) + sz;
+    } else {
+        const T sx = fmaT(w.m2[0], s.xm2, fmaT(w.m1[0], s.xm1, fmaT(w.p1[0], s.xp1, w.p2[0] * s.xp2)));
+        const T sy = fmaT(w.m2[1], s.ym2, fmaT(w.m1[1], s.ym1, fmaT(w.p1[1], s.yp1, w.p2[1] * s.yp2)));
+        const T sz = fmaT(w.m2[2], s.zm2, fmaT(w.m1[2], s.zm1, fmaT(w.p1[2], s.zp1, w.p2[2] * s.zp2)));
+        return fmaT(w.c, s.c, (sx + sy) + sz);
+    }
 }
 
 // The accumulator terms of the low-storage RK4 step recovered from stage

@@ -122,14 +122,16 @@ def _run_pinned_parareal(sp, name, tune_like_batch):
         # FP32 G acts on the FP64 increment only: its rounding differs from the
         # oracle's literal FP32 order far below the 1e-8 target
         _check_field(conv, fq, pin, f"iter{k_expect}", 1e-9)
-        # per-iteration errors and defects: 5 % where they are far above the FP32
-        # increment's rounding, which leaves ~1e-12 relative in the iterate.  The
-        # first defect is measured against the FP32 predictor itself, whose
-        # rounding (FMA contraction on the GPU, none in the oracle) differs by
-        # a few FP32 units (~1e-7 relative) between the two
+        # per-iteration errors and defects: 5 %, above a floor set by FP32 rounding.
+        # The coarse propagator rounds differently here (FMA contraction, the
+        # stencil as differences from the centre) and in the oracle (the
+        # reference's expressions, one rounding per operation): the iterates
+        # carry ~1e-11 relative of that difference through the coarse
+        # increments, and the first defect, measured against the FP32 predictor
+        # itself, ~1e-7
         for k in range(k_expect):
-            assert abs(rep["err_l2"][k] - err_l2[k]) <= 0.05 * err_l2[k] + 5e-12, (rule, k, rep["err_l2"], err_l2)
-            floor = 4e-7 if k == 0 else 5e-12
+            assert abs(rep["err_l2"][k] - err_l2[k]) <= 0.05 * err_l2[k] + 5e-11, (rule, k, rep["err_l2"], err_l2)
+            floor = 4e-7 if k == 0 else 5e-11
             assert abs(rep["defect"][k] - defect[k]) <= 0.05 * defect[k] + floor, (rule, k, rep["defect"], defect)
     return pin
 

@@ -169,3 +169,29 @@ def test_gpu_error_metric_matches_reference_definition(sp, orc):
     em, el = c.errors(fa, fb)
     assert abs(em - orc.error_maxrel(a, b)) < 1e-15
     assert abs(el - orc.error_l2rel(a, b)) < 1e-14
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_fp32_coarse_has_no_drift(sp, orc, n):
+    """The FP32 coarse propagator against FP64 over 28 steps of the one-GPU Parareal
+    workload's coarse step (dt = 0.2/224, nu = 0.01): no worse than twice the
+    oracle's own FP32 restatement (the stencil's weights, rounded to FP32, must not
+    act on the O(1) field values themselves, or every field drifts)."""
+    q0 = gaussian_noise(n, seed=0)
+    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0)
+    conv.autotune(sp.SP_F32, 1)
+    fin, fout = conv.field(sp.SP_F32), conv.field(sp.SP_F32)
+    conv.upload(fin, q0.astype(np.float32))
+    dt, steps = 0.2 / 224, 28
+    conv.DoRK4(fin, fout, 0.0, dt, steps)
+    got = conv.download(fout).astype(np.float64)
+    p = orc.params(n, nu0=0.01)
+    ref64 = orc.rk4(p, q0, 0.0, dt, steps)
+    ref32 = orc.rk4_f32(p, q0.astype(np.float32), 0.0, dt, steps).astype(np.float64)
+    assert rel_l2(got, ref64) < max(2.0 * rel_l2(ref32, ref64), 2e-7), (rel_l2(got, ref64), rel_l2(ref32, ref64))
+    # Euler in FP32 likewise
+    conv.DoEuler(fin, fout, 0.0, 1e-4, steps)
+    e64 = orc.euler(p, q0, 0.0, 1e-4, steps)
+    e32 = orc.euler_f32(p, q0.astype(np.float32), 0.0, 1e-4, steps).astype(np.float64)
+    eg = conv.download(fout).astype(np.float64)
+    assert rel_l2(eg, e64) < max(2.0 * rel_l2(e32, e64), 2e-7), (rel_l2(eg, e64), rel_l2(e32, e64))
