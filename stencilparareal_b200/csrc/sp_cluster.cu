@@ -57,56 +57,6 @@ struct ClusterArgs {
     StoreBounds sb;
 };
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_size() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-    return r;
-}
-// All threads of all CTAs of the cluster (hardware barrier, like __syncthreads).
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// Shared-memory address of the same variable in CTA `rank` of the cluster.
-__device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
-    return r;
-}
-// 16 bytes into another CTA's shared memory; the store counts its bytes off
-// the transaction count of that CTA's mbarrier `rbar` when it lands.
-__device__ __forceinline__ void st_async2(uint32_t addr, const V2& v, uint32_t rbar) {
-    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(addr),
-                 "d"(v.v[0]), "d"(v.v[1]), "r"(rbar)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx_u32(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t addr, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint32_t addr, uint32_t parity) {
-    if (mbar_try_wait_cluster(addr, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait_cluster(addr, parity)) return true;
-        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
-    }
-}
-
 // Cluster of C = nk / NZ CTAs per field (NZ >= 2, C >= 2); UPT units of two
 // x-adjacent cells of one row per thread, every own plane of each unit.
 template <int NZ, int UPT>
