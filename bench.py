@@ -323,7 +323,7 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
             # the cluster-resident path or the fused stage pairs when the tuner
             # preferred them, else the stage kernels' shape
             t64 = (a64["cluster"] if a64["cluster"]["kind"] == 3 else
-                   a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"])
+                   a64["P12"] if a64["P12"]["kind"] in (2, 4) else a64["S2"])
             tunes[n] = (t64, conv.autotune(sp.SP_F32, 1)["S2"])
         t64, t32 = tunes[n]
         conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])

@@ -269,7 +269,8 @@ long long sp_launch_count(void);
  * S1..S4, 4 = Euler): tile rows ty, z-chunk, kernel kind (0 direct loads, 1
  * TMA/mbarrier pipeline).  op 9 and 10: the fused stage pairs 1+2 and 3+4 of
  * FP64 RK4 steps: tile rows, planes per CTA (0 = one range per resident CTA),
- * kind 2 when RK4 steps run as fused pairs, else 0.  op 11: kind 3 when FP64 RK4
+ * kind 2 when RK4 steps run as fused pairs (4: on 32-column tiles), else 0.
+ * op 11: kind 3 when FP64 RK4
  * propagations run cluster-resident (sp_set_tune kind 3), else 0. */
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* kind);
 /* Runs the autotuner for this handle's grid at `batch` fields and precision: every
@@ -306,7 +307,9 @@ int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, 
 /* Forces one launch shape for a precision and batch.  kind 0 or 1: every
  * single-stage kernel, ty in {4,8,16}, zchunk >= 1, RK4 steps unfused.  kind 2
  * (FP64): RK4 steps as fused pairs with ty in {8,16} and zchunk planes per CTA
- * (0 = automatic).  kind 3 (FP64, small fields): every RK4 step of a DoRK4
+ * (0 = automatic) on tiles of 64 columns; kind 4 the same on tiles of 32 x 16
+ * cells (ty = 16; no wasted columns on grids such as 96^3).
+ * kind 3 (FP64, small fields): every RK4 step of a DoRK4
  * call (or of a Parareal fine sweep) in one launch, each field held in the
  * shared memory of a thread-block cluster (ty and zchunk unused; needs an even
  * ni, at most 2048 cells per plane and nk = C x {2,3,4} with 2 <= C <= 16). */

@@ -134,9 +134,10 @@ __device__ __forceinline__ void rhs_s(const W13<double>& wt, uint32_t at, const 
     }
 }
 
-template <int TY, int NSQ, int NP, int PAIR>
+template <int TY, int NSQ, int NP, int PAIR, int TXP = 64>
 struct PairShape {
-    static constexpr int TX = 64;
+    static constexpr int TX = TXP;                  // tile columns: 64 (one row per warp) or 32 (two)
+    static constexpr int NT = TY * TX / 2;          // threads: two cells of one tile row each
     static constexpr int WB = TX + 8, HB = TY + 8;  // stencil-input slot (box at x0-4, y0-4)
     static constexpr int WE = TX + 4, HE = TY + 4;  // widened first-stage slot (origin x0-2, y0-2)
     static constexpr int SB = WB * HB, SE = WE * HE, SA = TX * TY;
@@ -147,16 +148,16 @@ struct PairShape {
     static constexpr size_t smem = 128 + (size_t)(NSQ * SB + NE * SE + NP * SP) * 8 + (NSQ + NP) * 8;
 };
 
-template <int PAIR, int TY, int NSQ, int NP>
-__global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
+template <int PAIR, int TY, int NSQ, int NP, int TXP = 64>
+__global__ void __launch_bounds__(TY * TXP / 2, TY * TXP / 2 <= 256 ? 2 : 1)
     k_rk4_pair(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_q,
                const __grid_constant__ CUtensorMap tm_a, const PairArgs a) {
-    using S = PairShape<TY, NSQ, NP, PAIR>;
+    using S = PairShape<TY, NSQ, NP, PAIR, TXP>;
     constexpr int TX = S::TX, WB = S::WB, WE = S::WE, SB = S::SB, SE = S::SE, SP = S::SP;
     constexpr int NE = S::NE, NHR = S::NHR, NH = S::NH;
     constexpr uint32_t SBYTES = SB * 8, PBYTES = SP * 8;
     static_assert(SBYTES % 128 == 0 && (SE * 8) % 128 == 0 && (S::SA * 8) % 128 == 0, "slot alignment");
-    static_assert(NH <= 32 * TY, "ring chunks per CTA");
+    static_assert(NH <= S::NT, "ring chunks per CTA");
     static_assert(NSQ >= 6, "five stencil planes in use plus one in flight");
 
     extern __shared__ unsigned char smem_raw[];
@@ -165,7 +166,8 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     double* ps = es + NE * SE;
     uint64_t* bar = reinterpret_cast<uint64_t*>(ps + NP * SP);
 
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // thread -> cells (x0 + 2 px, x0 + 2 px + 1) of tile row `row`
+    const int tid = threadIdx.x, px = tid % (TX / 2), row = tid / (TX / 2);
     const bool leader = tid == 0;
 
     pdl_trigger();  // the next kernel's CTAs may start as this grid's CTAs retire
@@ -185,18 +187,18 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
     // not operands of the second stage)
     int hex = 0, hey = 0;
     if (tid < NHR) {
-        const int r = tid >> 5;
+        const int r = tid / (TX / 2);
         hey = r < 2 ? r : TY + r;
-        hex = 2 + 2 * (tid & 31);
+        hex = 2 + 2 * (tid % (TX / 2));
     } else if (has_h) {
         const int d = tid - NHR;
         hey = 2 + (d >> 1);
         hex = (d & 1) ? WE - 2 : 0;
     }
     // byte offsets in the slots
-    const uint32_t m_s8 = ((w + 4) * WB + 2 * lane + 4) * 8;
-    const uint32_t m_e8 = ((w + 2) * WE + 2 * lane + 2) * 8;
-    [[maybe_unused]] const uint32_t m_a8 = (w * TX + 2 * lane) * 8;
+    const uint32_t m_s8 = ((row + 4) * WB + 2 * px + 4) * 8;
+    const uint32_t m_e8 = ((row + 2) * WE + 2 * px + 2) * 8;
+    [[maybe_unused]] const uint32_t m_a8 = (row * TX + 2 * px) * 8;
     const uint32_t h_s8 = ((hey + 2) * WB + hex + 2) * 8;
     const uint32_t h_e8 = (hey * WE + hex) * 8;
     constexpr uint32_t EBYTES = SE * 8;
@@ -285,8 +287,8 @@ __global__ void __launch_bounds__(32 * TY, TY <= 8 ? 2 : 1)
 #pragma unroll
         for (int u = 0; u < 5; ++u) ew[u] = aw[u] = V2{};
 
-        const int x = x0 + 2 * lane;
-        const int y = y0 + w;
+        const int x = x0 + 2 * px;
+        const int y = y0 + row;
         const bool live = x < a.ni && y < a.nj;
         const bool full = x + 2 <= a.ni;
         // whether the cells have periodic images in x or y (image depth hd)
@@ -495,10 +497,10 @@ __global__ void k_widen(double* dst, Geo gd, const double* src, Geo gs, int item
     }
 }
 
-template <int PAIR, int TY, int NSQ, int NP>
+template <int PAIR, int TY, int NSQ, int NP, int TXP>
 cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, const Shape& sh, cudaStream_t s,
                           int* err) {
-    using S = PairShape<TY, NSQ, NP, PAIR>;
+    using S = PairShape<TY, NSQ, NP, PAIR, TXP>;
     CUtensorMap ts{}, tq{}, ta{};
     if (!make_tmap(&ts, g4, PAIR == 0 ? L.q : L.y2, L.items, S::WB, S::HB)) return cudaErrorInvalidValue;
     if (PAIR == 1) {
@@ -524,7 +526,7 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
         if (ctas_dev == 0) {
             int sms = 0, occ = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP>, 32 * TY, S::smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_pair<PAIR, TY, NSQ, NP, TXP>, S::NT, S::smem);
             ctas_dev = std::max(1, sms) * std::max(1, occ);
             if (dev >= 0 && dev < 64) cached[dev].store(ctas_dev, std::memory_order_relaxed);
         }
@@ -552,13 +554,13 @@ cudaError_t launch_pair_T(const Geo& g4, const Geo& go, const PairLaunch& L, con
     const long long nct = (total + a.span - 1) / a.span * a.cy;
     if (nct > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     const dim3 grid((unsigned)nct);
-    return launch_pdl(k_rk4_pair<PAIR, TY, NSQ, NP>, grid, dim3(32 * TY), S::smem, s, ts, tq, ta, a);
+    return launch_pdl(k_rk4_pair<PAIR, TY, NSQ, NP, TXP>, grid, dim3(S::NT), S::smem, s, ts, tq, ta, a);
 }
 
-template <int PAIR, int TY, int NSQ, int NP>
+template <int PAIR, int TY, int NSQ, int NP, int TXP = 64>
 cudaError_t set_pair_attr() {
-    return cudaFuncSetAttribute(k_rk4_pair<PAIR, TY, NSQ, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)PairShape<TY, NSQ, NP, PAIR>::smem);
+    return cudaFuncSetAttribute(k_rk4_pair<PAIR, TY, NSQ, NP, TXP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)PairShape<TY, NSQ, NP, PAIR, TXP>::smem);
 }
 
 unsigned grid_cells(long long n) {
@@ -583,6 +585,8 @@ cudaError_t prepare_pairs() {
     if (e == cudaSuccess) e = set_pair_attr<1, 8, 7, 2>();
     if (e == cudaSuccess) e = set_pair_attr<0, 16, 7, 2>();
     if (e == cudaSuccess) e = set_pair_attr<1, 16, 7, 2>();
+    if (e == cudaSuccess) e = set_pair_attr<0, 16, 7, 2, 32>();
+    if (e == cudaSuccess) e = set_pair_attr<1, 16, 7, 2, 32>();
     return e;
 }
 
@@ -590,12 +594,17 @@ cudaError_t launch_pair(const Geo& g4, const Geo& go, const PairLaunch& L, const
                         int* err) {
     add_launches(1);
     if (!pair_supported(g4) || g4.halo != 4 || sh.zchunk < 0) return cudaErrorInvalidValue;
+    // tile 64 x 8, 64 x 16 (one row per warp) or 32 x 16 (two rows per warp)
+    const bool narrow = sh.tx == 32;
+    if (narrow && sh.ty != 16) return cudaErrorInvalidValue;
     if (L.pair == 0) {
-        if (sh.ty == 8) return launch_pair_T<0, 8, 7, 2>(g4, go, L, sh, s, err);
-        if (sh.ty == 16) return launch_pair_T<0, 16, 7, 2>(g4, go, L, sh, s, err);
+        if (narrow) return launch_pair_T<0, 16, 7, 2, 32>(g4, go, L, sh, s, err);
+        if (sh.ty == 8) return launch_pair_T<0, 8, 7, 2, 64>(g4, go, L, sh, s, err);
+        if (sh.ty == 16) return launch_pair_T<0, 16, 7, 2, 64>(g4, go, L, sh, s, err);
     } else {
-        if (sh.ty == 8) return launch_pair_T<1, 8, 7, 2>(g4, go, L, sh, s, err);
-        if (sh.ty == 16) return launch_pair_T<1, 16, 7, 2>(g4, go, L, sh, s, err);
+        if (narrow) return launch_pair_T<1, 16, 7, 2, 32>(g4, go, L, sh, s, err);
+        if (sh.ty == 8) return launch_pair_T<1, 8, 7, 2, 64>(g4, go, L, sh, s, err);
+        if (sh.ty == 16) return launch_pair_T<1, 16, 7, 2, 64>(g4, go, L, sh, s, err);
     }
     return cudaErrorInvalidValue;
 }

@@ -35,6 +35,7 @@ struct Shape {
     int ty = 4;       // rows of a CTA tile
     int zchunk = 8;   // planes marched by one CTA
     int tma = 1;      // 1: TMA/mbarrier pipeline kernel; 0: direct-load kernel
+    int tx = 64;      // fused pairs: tile columns (64, or 32 with two tile rows per warp)
 };
 
 // Launch shapes of all stage kernels (indexed by Op, adjoint stages included).

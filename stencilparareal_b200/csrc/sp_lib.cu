@@ -559,8 +559,9 @@ int sp_convection_synchronize(sp_convection* h) {
 
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
-    if (kind < 0 || kind > 3)
-        return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA), 2 (fused pairs) or 3 (cluster-resident)");
+    if (kind < 0 || kind > 4)
+        return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA), 2 (fused pairs), 3 (cluster-resident) "
+                                    "or 4 (fused pairs on 32-column tiles)");
     if (kind == 3) {
         if (precision != SP_F64 || !cluster_supported(h->g[0]))
             return fail(SP_ERR_INVALID, "the cluster-resident path needs FP64, an even ni, small planes and nk = C x "
@@ -571,16 +572,18 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
         h->drop_graphs();
         return SP_OK;
     }
-    if (zchunk < (kind == 2 ? 0 : 1))
+    if (zchunk < (kind == 2 || kind == 4 ? 0 : 1))
         return fail(SP_ERR_INVALID, "zchunk must be >= 1 (>= 0 for fused pairs: planes per CTA, 0 = automatic)");
-    if (kind == 2) {
+    if (kind == 2 || kind == 4) {
         if (precision != SP_F64 || !pair_supported(h->g4))
             return fail(SP_ERR_INVALID, "fused stage pairs need FP64 and at least 4 cells per axis");
-        if (ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "fused pairs: ty must be 8 or 16");
+        if (kind == 2 && ty != 8 && ty != 16) return fail(SP_ERR_INVALID, "fused pairs: ty must be 8 or 16");
+        if (kind == 4 && ty != 16) return fail(SP_ERR_INVALID, "fused pairs on 32-column tiles: ty must be 16");
         Tune t = h->tune(precision, batch);
         Shape sh;
         sh.ty = ty;
         sh.zchunk = zchunk;
+        sh.tx = kind == 4 ? 32 : 64;
         t.pair[0] = t.pair[1] = sh;
         t.fused = 1;
         h->tunes[{precision, batch}] = t;
@@ -601,7 +604,8 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
 }
 
 // op 0..8: single-stage kernels (tma: 0 direct, 1 TMA); op 9, 10: fused pairs
-// 1+2 and 3+4 (tma: 2 when RK4 steps run fused, else 0); op 11: the
+// 1+2 and 3+4 (tma: 2 when RK4 steps run fused, 4 when fused on 32-column
+// tiles, else 0); op 11: the
 // cluster-resident path (tma: 3 when FP64 RK4 propagations use it, else 0).
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* tma) {
     if (!h) return fail(SP_ERR_INVALID, "null handle");
@@ -610,7 +614,7 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
     int kind;
     if (op == kNumOps || op == kNumOps + 1) {
         t = tn.pair[op - kNumOps];
-        kind = tn.fused ? 2 : 0;
+        kind = tn.fused ? (t.tx == 32 ? 4 : 2) : 0;
     } else if (op == kNumOps + 2) {
         t = Shape{0, 0, 0};
         kind = tn.cluster ? 3 : 0;
@@ -944,11 +948,11 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 L.nu = h->P.nu0;
                 L.dt = 1e-9;
                 L.q = w; L.acc = w + wb; L.y2 = w + 2 * wb; L.out = w + wb;
-                for (int ty : {8, 16})
+                for (int ty : {8, 16, 32})  // 32: tiles of 32 x 16 cells
                     for (int zc : {0, 16, 24, 32, 48, 64}) {
                         if (zc > g.nk) continue;
                         Shape sh;
-                        sh.ty = ty; sh.zchunk = zc;
+                        sh.ty = ty == 32 ? 16 : ty; sh.tx = ty == 32 ? 32 : 64; sh.zchunk = zc;
                         cudaError_t e = launch_pair(g4, g4, L, sh, s, h->err.as<int>());
                         if (e != cudaSuccess) { cudaGetLastError(); continue; }
                         float ms = 1e30f;

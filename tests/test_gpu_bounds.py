@@ -39,7 +39,8 @@ sizes = [(17, 19, 23), (130, 66, 12), (4, 4, 4), (64, 8, 5), (5, 130, 9)] if ful
 for n in sizes:
     c = sp.Convection(*n, 1.0 / n[0], 0.02, 0.0, 1.0, -0.5, 0.25)
     q0 = gaussian_noise(*n, seed=1)
-    tunes = [(4, 8, 1), (16, 3, 1), (8, 5, 0), (8, 0, 2), (16, 2, 2)] if full else [(4, 8, 1), (8, 0, 2)]
+    tunes = ([(4, 8, 1), (16, 3, 1), (8, 5, 0), (8, 0, 2), (16, 2, 2), (16, 0, 4), (16, 3, 4)] if full
+             else [(4, 8, 1), (8, 0, 2), (16, 0, 4)])
     for tune in tunes:
         c.set_tune(sp.SP_F64, 1, *tune)
         fi, fo = c.field(), c.field()
@@ -52,7 +53,7 @@ for n in sizes:
         c.DoRK4(gi, go, 0.0, 1e-3, 2)
 if full:
     n, P = 20, 4
-    for tune in ((4, 8, 1), (8, 0, 2)):
+    for tune in ((4, 8, 1), (8, 0, 2), (16, 0, 4)):
         conv = sp.Convection(n, n, n, 1.0 / n, 0.05, 0.0, 1.0, 0.5, -0.25)
         conv.set_tune(sp.SP_F64, P, *tune)
         conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.01, timeStepsFine=80,

@@ -14,8 +14,8 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
 SIZES = [(32, 32, 32), (17, 19, 23), (70, 9, 13), (4, 4, 4), (130, 66, 40), (64, 8, 5), (5, 130, 9)]
-# (ty, zchunk) of both pairs
-PAIR_SHAPES = [(8, 16), (16, 5), (8, 1), (16, 64), (8, 3)]
+# (ty, zchunk, kind) of both pairs: kind 2 tiles of 64 columns, kind 4 of 32 x 16
+PAIR_SHAPES = [(8, 16, 2), (16, 5, 2), (8, 1, 2), (16, 64, 2), (8, 3, 2), (16, 0, 4), (16, 7, 4), (16, 1, 4)]
 SINGLE = (4, 8, 1)  # single-stage TMA kernels, 4-row tiles, z-chunk 8
 
 
@@ -60,7 +60,7 @@ def test_fused_equals_single_stage(sp, n, shape):
     c = make(sp, n)
     q0 = gaussian_noise(*n, seed=5)
     ref, _ = run(sp, c, q0, SINGLE, 7)
-    got, fout = run(sp, c, q0, (shape[0], shape[1], 2), 7)
+    got, fout = run(sp, c, q0, shape, 7)
     assert np.array_equal(got, ref)
     assert halo_images_ok(fout)
 
@@ -119,7 +119,7 @@ def test_fused_batch_autotune_picks_a_valid_shape(sp):
     c.set_tune(sp.SP_F64, 1, *SINGLE)
     c.DoRK4(fin, fout, 0.0, 1e-4, 3)
     ref = c.download(fout)
-    if cfg["P12"]["kind"] == 2:
+    if cfg["P12"]["kind"] in (2, 4):
         assert np.array_equal(got, ref)
     else:  # the tuner may pick direct-load stage kernels (difference form of the update)
         assert rel_l2(got, ref) < 1e-13
@@ -132,7 +132,7 @@ def test_parareal_fine_sweep_fused_equals_single_stage(sp, skip):
     skipped) gives the same fields with fused pairs as with single-stage kernels."""
     n, P = 20, 4
     outs = []
-    for tune in (SINGLE, (8, 0, 2)):
+    for tune in (SINGLE, (8, 0, 2), (16, 0, 4)):
         conv = sp.Convection(n, n, n, 1.0 / n, 0.05, 0.0, 1.0, 0.5, -0.25)
         conv.set_tune(sp.SP_F64, P, *tune)
         conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.02, timeStepsFine=160,
@@ -143,8 +143,9 @@ def test_parareal_fine_sweep_fused_equals_single_stage(sp, skip):
         par.DoParallel()
         outs.append(conv.download(fsol))
         cfg = conv.tuned_configs(sp.SP_F64, P)
-        assert cfg["P12"]["kind"] == (2 if tune[2] == 2 else 0)
-    assert np.array_equal(outs[0], outs[1])
+        assert cfg["P12"]["kind"] == (tune[2] if tune[2] in (2, 4) else 0)
+    for o in outs[1:]:
+        assert np.array_equal(outs[0], o)
 
 
 def test_batch_autotune_then_parareal_equals_single_stage(sp):
@@ -157,9 +158,9 @@ def test_batch_autotune_then_parareal_equals_single_stage(sp):
         conv = sp.Convection(n, n, n, 1.0 / n, 0.05, 0.0, 1.0, 0.5, -0.25)
         if tune == "auto":
             cfg = conv.autotune(sp.SP_F64, P)
-            assert cfg["P12"]["kind"] in (0, 2) and cfg["P12"]["ty"] in (8, 16)
+            assert cfg["P12"]["kind"] in (0, 2, 4) and cfg["P12"]["ty"] in (8, 16)
             # direct-load stage kernels evaluate R in the difference form: not bit for bit
-            bitwise = cfg["P12"]["kind"] == 2 or all(cfg[k]["kind"] == 1 for k in ("S1", "S2", "S3", "S4"))
+            bitwise = cfg["P12"]["kind"] in (2, 4) or all(cfg[k]["kind"] == 1 for k in ("S1", "S2", "S3", "S4"))
         else:
             conv.set_tune(sp.SP_F64, P, *tune)
         conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.05, gridSize=n, endTime=0.02, timeStepsFine=120,
@@ -192,3 +193,20 @@ def test_kernel_times_paths_leave_field_unchanged(sp):
     kp2 = c.kernel_times(f, 1e-4, reps=2, path="pairs")
     assert set(kp2) == {"P12", "P34"} and all(v > 0 for v in kp2.values())
     assert torch.equal(f.data, before)
+
+
+@pytest.mark.parametrize("n", [(96, 24, 20), (48, 48, 12), (33, 17, 9), (256, 16, 8)])
+def test_narrow_tiles_on_grids_of_odd_tile_counts(sp, orc, n):
+    """Tiles of 32 x 16 cells (sp_set_tune kind 4): grids whose width is not a multiple
+    of 64 (96, 48, odd), bit for bit with the single-stage kernels and with the
+    64-column tiles, across a graph chunk and in place."""
+    c = make(sp, n)
+    q0 = gaussian_noise(*n, seed=17)
+    a, _ = run(sp, c, q0, SINGLE, 53)
+    b, fb = run(sp, c, q0, (16, 0, 4), 53)
+    d, _ = run(sp, c, q0, (16, 0, 4), 53, inplace=True)
+    e, _ = run(sp, c, q0, (8, 0, 2), 53)
+    assert np.array_equal(a, b) and np.array_equal(a, d) and np.array_equal(a, e)
+    assert halo_images_ok(fb)
+    p = orc.params(n, dx=1.0 / n[0], nu0=0.02, cx=1.0, cy=-0.5, cz=0.25)
+    assert rel_l2(b, orc.rk4(p, q0, 0.0, 1e-4, 53)) < TOL64

@@ -90,7 +90,8 @@ def _run_pinned_parareal(sp, name, tune_like_batch):
     if tune_like_batch:
         # the batch benchmark's tuning: the batched tune of 16 fields applied to P
         a64 = conv.autotune(sp.SP_F64, 16)
-        t64 = a64["cluster"] if a64["cluster"]["kind"] == 3 else a64["P12"] if a64["P12"]["kind"] == 2 else a64["S2"]
+        t64 = (a64["cluster"] if a64["cluster"]["kind"] == 3 else
+               a64["P12"] if a64["P12"]["kind"] in (2, 4) else a64["S2"])
         t32 = conv.autotune(sp.SP_F32, 1)["S2"]
         conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
         conv.set_tune(sp.SP_F32, 1, t32["ty"], t32["zchunk"], t32["kind"])
