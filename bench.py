@@ -652,7 +652,11 @@ def main():
                          "frac_in_step": alg_launch / (dom_in_step * 1e-3) / 1e9 / peak,
                          "in_step_note": "timed region's step time x the kernel's share of the event-timed "
                                          "kernel times (launches overlap through programmatic dependent "
-                                         "launch inside the step)"},
+                                         "launch inside the step)",
+                         # the whole step against the reference scheme's own traffic: 16 FP64 field
+                         # accesses per cell-update (128 B) for its low-storage stage sequence
+                         "step_equiv_128B_gbs": 128 * value / world,
+                         "step_equiv_128B_frac": 128 * value / world / peak},
             "roofline_single_stage": roofline_single,
             "roofline_fused_pairs": roofline_pairs,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
