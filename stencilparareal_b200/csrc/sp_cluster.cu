@@ -100,6 +100,32 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
         ux[j] = uv[j] ? 2 * (u % half) : 0;
         uy[j] = uv[j] ? u / half : 0;
     }
+    const uint32_t plane_bytes = (uint32_t)plane_cells * 8u;
+    // byte offsets inside a plane of a unit's cells and of their x- and
+    // y-neighbours (periodic): computed once per launch with one unit and up
+    // to 3 planes per thread, per stage otherwise (where keeping them would
+    // spill registers)
+    constexpr bool kKeep = UPT == 1 && NZ < 4;
+    // with one unit and two planes per thread, the stage values sent to the
+    // neighbours stay in registers instead of being read back after the barrier
+    constexpr bool kSendRegs = UPT == 1 && NZ == 2;
+    struct Offs {
+        uint32_t c, l, r, ym2, ym1, yp1, yp2;
+    };
+    auto offsets = [&](int j) {
+        const int x = ux[j], y = uy[j];
+        Offs o;
+        o.c = (uint32_t)((y * ni + x) * 8);
+        o.l = (uint32_t)((y * ni + (x + ni - 2) % ni) * 8);
+        o.r = (uint32_t)((y * ni + (x + 2) % ni) * 8);
+        o.ym2 = (uint32_t)((((y + nj - 2) % nj) * ni + x) * 8);
+        o.ym1 = (uint32_t)((((y + nj - 1) % nj) * ni + x) * 8);
+        o.yp1 = (uint32_t)((((y + 1) % nj) * ni + x) * 8);
+        o.yp2 = (uint32_t)((((y + 2) % nj) * ni + x) * 8);
+        return o;
+    };
+    [[maybe_unused]] Offs off1{};
+    if constexpr (kKeep) off1 = offsets(0);
     // load: own planes into registers and buffer 0; the four halo planes of
     // buffer 0 from the field's interior (periodic in z)
     V2 q[UPT][NZ], acc[UPT][NZ];
@@ -139,26 +165,27 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
         const bool exchange = g + 1 < nstage;  // the last stage's output goes to global memory only
         const uint32_t nbar = bar0 + 8u * (uint32_t)((g + 1) & 1);  // completes when stage g+1's halo has landed
         if (exchange && tid == 0) mbar_arrive_expect_tx_u32(nbar, halo_bytes);
+        [[maybe_unused]] V2 sendv[NZ];
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             if (!uv[j]) continue;
-            const int x = ux[j], y = uy[j];
-            const int xl = (x + ni - 2) % ni, xr = (x + 2) % ni;
-            const int ym1 = (y + nj - 1) % nj, ym2 = (y + nj - 2) % nj, yp1 = (y + 1) % nj, yp2 = (y + 2) % nj;
+            Offs of;
+            if constexpr (kKeep) of = off1;
+            else of = offsets(j);
             // the unit's column of stage inputs: planes -2 .. NZ+1 (z-window)
             V2 col[NPL];
 #pragma unroll
-            for (int p = 0; p < NPL; ++p) col[p] = lds2(src + (uint32_t)((p * plane_cells + y * ni + x) * 8));
+            for (int p = 0; p < NPL; ++p) col[p] = lds2(src + (uint32_t)p * plane_bytes + of.c);
 #pragma unroll
             for (int o = 0; o < NZ; ++o) {
                 const int p = o + 2;
-                const uint32_t row = src + (uint32_t)(p * plane_cells * 8);
-                const V2 L = lds2(row + (uint32_t)((y * ni + xl) * 8));
-                const V2 R = lds2(row + (uint32_t)((y * ni + xr) * 8));
-                const V2 Ym1 = lds2(row + (uint32_t)((ym1 * ni + x) * 8));
-                const V2 Ym2 = lds2(row + (uint32_t)((ym2 * ni + x) * 8));
-                const V2 Yp1 = lds2(row + (uint32_t)((yp1 * ni + x) * 8));
-                const V2 Yp2 = lds2(row + (uint32_t)((yp2 * ni + x) * 8));
+                const uint32_t row = src + (uint32_t)p * plane_bytes;
+                const V2 L = lds2(row + of.l);
+                const V2 R = lds2(row + of.r);
+                const V2 Ym1 = lds2(row + of.ym1);
+                const V2 Ym2 = lds2(row + of.ym2);
+                const V2 Yp1 = lds2(row + of.yp1);
+                const V2 Yp2 = lds2(row + of.yp2);
                 const V2& cen = col[p];
                 const double rowv[6] = {L.v[0], L.v[1], cen.v[0], cen.v[1], R.v[0], R.v[1]};
                 V2 out;
@@ -185,8 +212,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
                     }
                 }
                 if constexpr (ST == 3) q[j][o] = out;
-                const uint32_t cell = (uint32_t)((y * ni + x) * 8);
-                sts2(dst + (uint32_t)(p * plane_cells * 8) + cell, out);
+                if constexpr (kSendRegs) sendv[o] = out;
+                sts2(dst + (uint32_t)p * plane_bytes + of.c, out);
             }
         }
         // own planes of dst written before the next stage reads them, and every
@@ -199,16 +226,18 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
 #pragma unroll
             for (int j = 0; j < UPT; ++j) {
                 if (!uv[j]) continue;
-                const uint32_t cell = (uint32_t)((uy[j] * ni + ux[j]) * 8);
+                const uint32_t cell = kKeep ? off1.c : offsets(j).c;
 #pragma unroll
                 for (int o = 0; o < NZ; ++o) {
                     if (o >= 2 && o < NZ - 2) continue;
-                    const V2 v = lds2(dst + (uint32_t)((o + 2) * plane_cells * 8) + cell);
+                    V2 v;
+                    if constexpr (kSendRegs) v = sendv[o];
+                    else v = lds2(dst + (uint32_t)(o + 2) * plane_bytes + cell);
                     if (o < 2)
-                        st_async2(map_rank(dst + (uint32_t)((NZ + 2 + o) * plane_cells * 8) + cell, lower), v,
+                        st_async2(map_rank(dst + (uint32_t)(NZ + 2 + o) * plane_bytes + cell, lower), v,
                                   map_rank(nbar, lower));
                     if (o >= NZ - 2)
-                        st_async2(map_rank(dst + (uint32_t)((o - (NZ - 2)) * plane_cells * 8) + cell, upper), v,
+                        st_async2(map_rank(dst + (uint32_t)(o - (NZ - 2)) * plane_bytes + cell, upper), v,
                                   map_rank(nbar, upper));
                 }
             }
