@@ -156,6 +156,24 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
         constexpr int ST = decltype(stc)::value;
         const uint32_t src = base0 + (uint32_t)(g & 1) * buf_bytes;
         const uint32_t dst = base0 + (uint32_t)((g + 1) & 1) * buf_bytes;
+        // NZ = 2, one unit: the first own plane's operands (centre, x- and
+        // y-neighbours; written by this CTA before the last barrier) are loaded
+        // before the wait for the halo planes (an invalid unit reads cell 0;
+        // the second plane's as well would spill registers)
+        [[maybe_unused]] V2 pre[1][7];
+        if constexpr (kSendRegs) {
+#pragma unroll
+            for (int o = 0; o < 1; ++o) {
+                const uint32_t row = src + (uint32_t)(o + 2) * plane_bytes;
+                pre[o][0] = lds2(row + off1.c);
+                pre[o][1] = lds2(row + off1.l);
+                pre[o][2] = lds2(row + off1.r);
+                pre[o][3] = lds2(row + off1.ym1);
+                pre[o][4] = lds2(row + off1.ym2);
+                pre[o][5] = lds2(row + off1.yp1);
+                pre[o][6] = lds2(row + off1.yp2);
+            }
+        }
         if (g > 0 && !bad) {
             // halo planes of this stage's input, written by both z-neighbours at the
             // end of stage g-1 (after one wait has given up, none is tried again:
@@ -175,17 +193,27 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
             // the unit's column of stage inputs: planes -2 .. NZ+1 (z-window)
             V2 col[NPL];
 #pragma unroll
-            for (int p = 0; p < NPL; ++p) col[p] = lds2(src + (uint32_t)p * plane_bytes + of.c);
+            for (int p = 0; p < NPL; ++p) {
+                if constexpr (kSendRegs) {
+                    if (p == 2) { col[p] = pre[0][0]; continue; }
+                }
+                col[p] = lds2(src + (uint32_t)p * plane_bytes + of.c);
+            }
 #pragma unroll
             for (int o = 0; o < NZ; ++o) {
                 const int p = o + 2;
                 const uint32_t row = src + (uint32_t)p * plane_bytes;
-                const V2 L = lds2(row + of.l);
-                const V2 R = lds2(row + of.r);
-                const V2 Ym1 = lds2(row + of.ym1);
-                const V2 Ym2 = lds2(row + of.ym2);
-                const V2 Yp1 = lds2(row + of.yp1);
-                const V2 Yp2 = lds2(row + of.yp2);
+                V2 L, R, Ym1, Ym2, Yp1, Yp2;
+                if (kSendRegs && o == 0) {
+                    L = pre[0][1]; R = pre[0][2]; Ym1 = pre[0][3]; Ym2 = pre[0][4]; Yp1 = pre[0][5]; Yp2 = pre[0][6];
+                } else {
+                    L = lds2(row + of.l);
+                    R = lds2(row + of.r);
+                    Ym1 = lds2(row + of.ym1);
+                    Ym2 = lds2(row + of.ym2);
+                    Yp1 = lds2(row + of.yp1);
+                    Yp2 = lds2(row + of.yp2);
+                }
                 const V2& cen = col[p];
                 const double rowv[6] = {L.v[0], L.v[1], cen.v[0], cen.v[1], R.v[0], R.v[1]};
                 V2 out;
