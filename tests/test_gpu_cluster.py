@@ -89,11 +89,13 @@ def test_autotuner_considers_cluster_path_and_unsupported_grids_are_refused(sp):
         big.set_tune(sp.SP_F64, 1, 0, 0, 3)
 
 
-@pytest.mark.parametrize("skip", [True, False])
-def test_parareal_fine_sweep_on_clusters_equals_stage_kernels(sp, skip):
+@pytest.mark.parametrize("skip,P", [(True, 6), (False, 6), (True, 40)])
+def test_parareal_fine_sweep_on_clusters_equals_stage_kernels(sp, skip, P):
     """All slices' fine runs of a Parareal iteration in one launch, one cluster per
-    slice (converged slices gated off on the device)."""
-    n, P = 16, 6
+    slice (converged slices gated off on the device).  With 40 slices the clusters
+    of 2 planes per CTA (8 CTAs each) would exceed the SMs, so the batch runs
+    clusters of 4 planes per CTA."""
+    n = 16
     outs = []
     for kind in (1, 3):
         conv = sp.Convection(n, n, n, 1.0 / n, 0.02, 0.0, 1.0, -0.5, 0.25)
@@ -101,8 +103,8 @@ def test_parareal_fine_sweep_on_clusters_equals_stage_kernels(sp, skip):
             conv.set_tune(sp.SP_F64, P, 0, 0, 3)
         else:
             conv.set_tune(sp.SP_F64, P, 4, 8, 1)
-        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.02, gridSize=n, endTime=0.03, timeStepsFine=240,
-                                       timeStepsCoarse=18, kmax=4)
+        conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.02, gridSize=n, endTime=0.03, timeStepsFine=6 * P * 7,
+                                       timeStepsCoarse=3 * P, kmax=4)
         fin, fsol = conv.field(), conv.field()
         conv.upload(fin, gaussian_noise(n, seed=5))
         rep = sp.Parareal(conv, fin, fsol, 0.0, conf, coarse="rk4", coarse_precision="f32",
