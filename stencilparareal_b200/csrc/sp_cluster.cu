@@ -10,15 +10,17 @@
 // start q and the accumulator of its cells in registers.  A stage reads the
 // 13-point star from shared memory (x and y wrap around inside the plane; z
 // from the halo planes), writes the next stage input into the other of two
-// shared buffers and, once all its threads are past the stage, stores its two
-// lowest / highest planes into the z-neighbours' halo planes with st.async
-// (the neighbours then start the next stage, which writes into the buffer
-// this stage read), each store counting its bytes off
-// the transaction count of the receiving CTA's mbarrier.  A CTA posts the halo
-// bytes it expects for the next stage, and waits (acquire, bounded by
-// %globaltimer) until they have landed: two neighbours per stage instead of a
-// barrier over the whole cluster, no fence and no separate arrival.  Nothing
-// goes to global memory between the first load and the last store.
+// shared buffers and stores each value of its two lowest / highest planes, as
+// soon as it is computed, into the z-neighbours' halo planes with st.async,
+// each store counting its bytes off the transaction count of the receiving
+// CTA's mbarrier.  A CTA posts the halo bytes it expects for the next stage,
+// and waits (acquire, bounded by %globaltimer) until they have landed: two
+// neighbours per stage instead of a barrier over the whole cluster, no fence
+// and no separate arrival.  The early stores are safe with two buffers: a
+// neighbour's next stage writes into the buffer this stage reads, but only
+// after it has received every value of this stage, and every thread sends
+// after all its reads (its values depend on them).  Nothing goes to global
+// memory between the first load and the last store.
 //
 // Every value is computed with the operations, and in the order, of the
 // single-stage kernels (rhs_w13 and the 13-access low-storage epilogues of
@@ -106,9 +108,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
     // to 3 planes per thread, per stage otherwise (where keeping them would
     // spill registers)
     constexpr bool kKeep = UPT == 1 && NZ < 4;
-    // with one unit and two planes per thread, the stage values sent to the
-    // neighbours stay in registers instead of being read back after the barrier
-    constexpr bool kSendRegs = UPT == 1 && NZ == 2;
+    // with one unit and two planes per thread, the first own plane's operands
+    // are loaded before the wait for the halo planes
+    constexpr bool kPreload = UPT == 1 && NZ == 2;
     struct Offs {
         uint32_t c, l, r, ym2, ym1, yp1, yp2;
     };
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
         // before the wait for the halo planes (an invalid unit reads cell 0;
         // the second plane's as well would spill registers)
         [[maybe_unused]] V2 pre[1][7];
-        if constexpr (kSendRegs) {
+        if constexpr (kPreload) {
 #pragma unroll
             for (int o = 0; o < 1; ++o) {
                 const uint32_t row = src + (uint32_t)(o + 2) * plane_bytes;
@@ -183,7 +185,6 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
         const bool exchange = g + 1 < nstage;  // the last stage's output goes to global memory only
         const uint32_t nbar = bar0 + 8u * (uint32_t)((g + 1) & 1);  // completes when stage g+1's halo has landed
         if (exchange && tid == 0) mbar_arrive_expect_tx_u32(nbar, halo_bytes);
-        [[maybe_unused]] V2 sendv[NZ];
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             if (!uv[j]) continue;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
             V2 col[NPL];
 #pragma unroll
             for (int p = 0; p < NPL; ++p) {
-                if constexpr (kSendRegs) {
+                if constexpr (kPreload) {
                     if (p == 2) { col[p] = pre[0][0]; continue; }
                 }
                 col[p] = lds2(src + (uint32_t)p * plane_bytes + of.c);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
                 const int p = o + 2;
                 const uint32_t row = src + (uint32_t)p * plane_bytes;
                 V2 L, R, Ym1, Ym2, Yp1, Yp2;
-                if (kSendRegs && o == 0) {
+                if (kPreload && o == 0) {
                     L = pre[0][1]; R = pre[0][2]; Ym1 = pre[0][3]; Ym2 = pre[0][4]; Yp1 = pre[0][5]; Yp2 = pre[0][6];
                 } else {
                     L = lds2(row + of.l);
@@ -240,36 +241,26 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
                     }
                 }
                 if constexpr (ST == 3) q[j][o] = out;
-                if constexpr (kSendRegs) sendv[o] = out;
                 sts2(dst + (uint32_t)p * plane_bytes + of.c, out);
-            }
-        }
-        // own planes of dst written before the next stage reads them, and every
-        // thread of this CTA done reading src: only then may the neighbours
-        // start the next stage, whose halo stores land in the buffer src is
-        __syncthreads();
-        if (exchange) {
-            // the lower neighbour's upper halo planes NZ+2, NZ+3 are our own planes 0, 1;
-            // the upper neighbour's lower halo planes 0, 1 our own planes NZ-2, NZ-1
-#pragma unroll
-            for (int j = 0; j < UPT; ++j) {
-                if (!uv[j]) continue;
-                const uint32_t cell = kKeep ? off1.c : offsets(j).c;
-#pragma unroll
-                for (int o = 0; o < NZ; ++o) {
-                    if (o >= 2 && o < NZ - 2) continue;
-                    V2 v;
-                    if constexpr (kSendRegs) v = sendv[o];
-                    else v = lds2(dst + (uint32_t)(o + 2) * plane_bytes + cell);
+                // the plane goes to the z-neighbours at once: the lower neighbour's
+                // upper halo planes NZ+2, NZ+3 are our own planes 0, 1; the upper
+                // neighbour's lower halo planes 0, 1 our own planes NZ-2, NZ-1.
+                // Every thread with a unit sends, each after all its reads of src
+                // (its values depend on them), and a neighbour writes into our src
+                // halo planes only once its next stage has every byte of ours.
+                if (exchange) {
                     if (o < 2)
-                        st_async2(map_rank(dst + (uint32_t)(NZ + 2 + o) * plane_bytes + cell, lower), v,
+                        st_async2(map_rank(dst + (uint32_t)(NZ + 2 + o) * plane_bytes + of.c, lower), out,
                                   map_rank(nbar, lower));
                     if (o >= NZ - 2)
-                        st_async2(map_rank(dst + (uint32_t)(o - (NZ - 2)) * plane_bytes + cell, upper), v,
+                        st_async2(map_rank(dst + (uint32_t)(o - (NZ - 2)) * plane_bytes + of.c, upper), out,
                                   map_rank(nbar, upper));
                 }
             }
         }
+        // own planes of dst written before the next stage reads them, and every
+        // thread of this CTA done reading src before the next stage overwrites it
+        __syncthreads();
     };
     for (int i = 0; i < a.nsteps; ++i) {
         if (a.wtab) w = a.wtab[i];
