@@ -608,15 +608,24 @@ def main():
     alg_launch = KERNEL_BYTES[dom] * n ** 3
     achieved = alg_launch / (ktimes[dom] * 1e-3) / 1e9
     step_bytes = sum(KERNEL_BYTES[k] for k in ktimes)
-    traffic_tab = {}
+    traffic_all = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                traffic_tab = json.load(f).get("dram_bytes_per_launch", {})
+                traffic_all = json.load(f)
         except Exception:
-            traffic_tab = {}
-    traffic = traffic_tab.get(dom)
+            traffic_all = {}
+
+    def traffic_of(k):
+        """ncu DRAM bytes per launch of kernel k as tuned (the pairs' traffic
+        depends on their tile and range length); None where none was measured."""
+        if k in ("P12", "P34"):
+            sh = tune.get(k, {})
+            tile = "32x16" if sh.get("kind") == 4 else f"64x{sh.get('ty', 8)}"
+            return traffic_all.get("pairs_by_shape", {}).get(f"{tile}/z{sh.get('zchunk', 0)}", {}).get(k)
+        return traffic_all.get("dram_bytes_per_launch", {}).get(k)
+    traffic = traffic_of(dom)
     # both paths on the same field, for comparison: the four single-stage kernels
     # move 104 B per cell-update and are bound by HBM; the fused pairs move 56 B
     # and are bound on chip
@@ -626,7 +635,7 @@ def main():
         sb = sum(KERNEL_BYTES[k] for k in kt)
         tot = sum(kt.values()) * 1e-3
         return {"bound": "hbm", "kernel": KERNEL_NAMES[d], "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "traffic": traffic_tab.get(d), "kernel_times_ms": kt,
+                "frac": ach / peak, "traffic": traffic_of(d), "kernel_times_ms": kt,
                 "algorithmic_bytes_per_cell_update": sb, "step_achieved_gbs": sb * n ** 3 / tot / 1e9,
                 "step_frac": sb * n ** 3 / tot / 1e9 / peak, "step_gcups_from_kernel_times": n ** 3 / tot / 1e9}
     roofline_single = path_roofline(conv.kernel_times(fin, DT, reps=20, path="stages"))

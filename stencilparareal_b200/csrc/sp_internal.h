@@ -37,6 +37,9 @@ struct Shape {
     int tma = 1;      // 1: TMA/mbarrier pipeline kernel; 0: direct-load kernel
     int tx = 64;      // fused pairs: tile columns (64, or 32 with two tile rows per warp)
 };
+inline bool same_shape(const Shape& a, const Shape& b) {
+    return a.ty == b.ty && a.zchunk == b.zchunk && a.tma == b.tma && a.tx == b.tx;
+}
 
 // Launch shapes of all stage kernels (indexed by Op, adjoint stages included).
 constexpr int kNumOps = OP_ADJ + 4;

@@ -359,6 +359,13 @@ constexpr float kPairMargin = 0.98f;
 // pairs) draw more: timed cold, they win by 1-3 %; sustained (the clocks at
 // ~1.55 GHz instead of ~1.9 GHz), the pairs are ~9 % faster at 256^3.
 constexpr double kSustainSeconds = 0.4;
+// The pairs on 32 x 16 tiles carry less halo per cell than on 64-column tiles
+// (TMA boxes of 40 x 24 against 72 x 16 cells per 512), so they move fewer DRAM
+// bytes and draw less power at the same speed per clock: where the cap bites
+// they keep a higher clock (256^3: 52.3 against 50.8 GCUPS on one box, equal
+// where neither path reaches the cap).  Timed at sustained clocks, they are kept
+// unless more than 1 % slower than the per-pair best of the isolated timings.
+constexpr float kNarrowMargin = 1.01f;
 
 // Runs fn back to back (synchronising after each) until kSustainSeconds have passed.
 template <typename F>
@@ -940,6 +947,8 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
         if (wbuf.alloc(3 * wb) == cudaSuccess) {
             char* w = wbuf.as<char>();
             float pair_ms[2] = {1e30f, 1e30f};
+            float narrow_ms[2] = {1e30f, 1e30f};  // the best shape on 32 x 16 tiles
+            Shape narrow[2];
             for (int pair = 0; pair < 2; ++pair) {
                 PairLaunch L;
                 L.pair = pair;
@@ -966,8 +975,16 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                             ms = std::min(ms, m);
                         }
                         if (ms < pair_ms[pair]) { pair_ms[pair] = ms; best.pair[pair] = sh; }
+                        if (ty == 32 && ms < narrow_ms[pair]) { narrow_ms[pair] = ms; narrow[pair] = sh; }
                     }
             }
+            // the pair shapes to compare at sustained clocks: the per-pair best and,
+            // when it differs, the best on 32 x 16 tiles for both pairs
+            Tune alt = best;
+            alt.pair[0] = narrow[0];
+            alt.pair[1] = narrow[1];
+            const bool try_narrow = narrow_ms[0] < 1e29f && narrow_ms[1] < 1e29f &&
+                                    !(same_shape(alt.pair[0], best.pair[0]) && same_shape(alt.pair[1], best.pair[1]));
             best.fused = (pair_ms[0] + pair_ms[1]) < (op_ms[OP_RK_S1] + op_ms[OP_RK_S2] + op_ms[OP_RK_S3] +
                                                       op_ms[OP_RK_S4]) ? 1 : 0;
             if (batch == 1) {
@@ -976,10 +993,10 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 // dependent launch and four stage kernels overlap more than two
                 // pairs, so that the sums of isolated kernel times mislead.
                 SP_CUDA(fill_wave(p, 2 * fb, g.es, s));
-                float path_ms[2] = {1e30f, 1e30f};
-                for (int f = 0; f < 2 && rc == SP_OK; ++f) {
-                    Tune tt = best;
-                    tt.fused = f;
+                float path_ms[3] = {1e30f, 1e30f, 1e30f};  // stages, best pairs, pairs on 32 x 16 tiles
+                for (int f = 0; f < (try_narrow ? 3 : 2) && rc == SP_OK; ++f) {
+                    Tune tt = f == 2 ? alt : best;
+                    tt.fused = f ? 1 : 0;
                     h->tunes[{precision, batch}] = tt;
                     h->drop_graphs();
                     rc = do_prop(h, precision, true, p, p + fb, 0.0, dtt, kChunk + 1);  // captures the graph
@@ -1001,6 +1018,11 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                     h->drop_graphs();
                     return rc;
                 }
+                if (try_narrow && path_ms[2] <= kNarrowMargin * path_ms[1]) {
+                    best.pair[0] = alt.pair[0];
+                    best.pair[1] = alt.pair[1];
+                    path_ms[1] = path_ms[2];
+                }
                 best.fused = path_ms[1] < kPairMargin * path_ms[0] ? 1 : 0;
             } else {
                 // Batches (the Parareal F sweep): four consecutive batched steps of
@@ -1018,30 +1040,32 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                                              p + 2 * fb, p + 3 * fb, batch, nullptr, 0, ts, s, err);
                     return x;
                 };
-                auto pair_steps = [&](int k) {
+                auto pair_steps = [&](const Tune& pt, int k) {
                     cudaError_t x = cudaSuccess;
                     for (int i = 0; i < k && x == cudaSuccess; ++i) {
                         char* Q = w + (size_t)(i % 2) * wb;
                         char* A = w + (size_t)((i + 1) % 2) * wb;
-                        x = enqueue_pair_step(h, best, dtt, nu, Q, A, w + 2 * wb, A, h->g4, batch, nullptr, 0, s,
-                                              err);
+                        x = enqueue_pair_step(h, pt, dtt, nu, Q, A, w + 2 * wb, A, h->g4, batch, nullptr, 0, s, err);
                     }
                     return x;
                 };
-                float path_ms[2] = {1e30f, 1e30f};
+                auto path_steps = [&](int f, int k) {
+                    return f == 0 ? stage_steps(k) : pair_steps(f == 2 ? alt : best, k);
+                };
+                float path_ms[3] = {1e30f, 1e30f, 1e30f};  // stages, best pairs, pairs on 32 x 16 tiles
                 cudaError_t x = cudaSuccess;
-                for (int f = 0; f < 2 && x == cudaSuccess; ++f) {
-                    x = f ? pair_steps(1) : stage_steps(1);
+                for (int f = 0; f < (try_narrow ? 3 : 2) && x == cudaSuccess; ++f) {
+                    x = path_steps(f, 1);
                     if (x == cudaSuccess) {  // at the clocks the path sustains
                         int rs = sustain(s, [&]() {
-                            cudaError_t y = f ? pair_steps(4) : stage_steps(4);
+                            cudaError_t y = path_steps(f, 4);
                             return y == cudaSuccess ? SP_OK : fail(SP_ERR_CUDA, "tuning: %s", cudaGetErrorString(y));
                         });
                         if (rs) x = cudaErrorUnknown;
                     }
                     for (int r = 0; r < 3 && x == cudaSuccess; ++r) {
                         cudaEventRecord(e0, s);
-                        x = f ? pair_steps(4) : stage_steps(4);
+                        x = path_steps(f, 4);
                         cudaEventRecord(e1, s);
                         cudaEventSynchronize(e1);
                         float m = 0;
@@ -1053,6 +1077,11 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                     cudaEventDestroy(e0);
                     cudaEventDestroy(e1);
                     return fail(SP_ERR_CUDA, "tuning batched steps: %s", cudaGetErrorString(x));
+                }
+                if (try_narrow && path_ms[2] <= kNarrowMargin * path_ms[1]) {
+                    best.pair[0] = alt.pair[0];
+                    best.pair[1] = alt.pair[1];
+                    path_ms[1] = path_ms[2];
                 }
                 best.fused = path_ms[1] < kPairMargin * path_ms[0] ? 1 : 0;
             }
