@@ -279,8 +279,12 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
  * stages: for batch 1 as timed through sp_do_rk4 (a graph chunk of 50 steps on
  * scratch fields), for larger batches over four consecutive batched steps, each
  * path timed after 0.4 s of running back to back (at the clocks it sustains
- * under the GPU's power cap).  Small FP64 fields then take the
- * cluster-resident path (kind 3 of sp_set_tune) when it is faster. */
+ * under the GPU's power cap).  The pairs' shapes are chosen per pair by
+ * isolated timing, then compared, in the same sustained way, with both pairs
+ * on their best 32 x 16 tiles, which are kept unless more than 1 % slower
+ * (they move fewer DRAM bytes, so they hold a higher clock under the cap).
+ * Small FP64 fields then take the cluster-resident path (kind 3 of
+ * sp_set_tune) when it is faster.  Takes about 1-3 s. */
 int sp_autotune(sp_convection* h, int precision, int batch);
 /* Test of the error path of the bounded in-kernel waits: runs one kernel whose
  * wait can never complete and gives up after limit_ms (<= 2000); returns
