@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-12
 SIZES = [(32, 32, 32), (17, 19, 23), (70, 9, 13), (4, 4, 4), (130, 66, 40), (64, 8, 5), (5, 130, 9)]
 # (ty, zchunk, kind) of both pairs: kind 2 tiles of 64 columns, kind 4 of 32 x 16
-PAIR_SHAPES = [(8, 16, 2), (16, 5, 2), (8, 1, 2), (16, 64, 2), (8, 3, 2), (16, 0, 4), (16, 7, 4), (16, 1, 4)]
+PAIR_SHAPES = [(8, 16, 2), (16, 5, 2), (8, 1, 2), (16, 64, 2), (8, 3, 2), (16, 0, 4), (16, 7, 4), (16, 1, 4),
+               (16, 64, 4), (16, 24, 4)]
 SINGLE = (4, 8, 1)  # single-stage TMA kernels, 4-row tiles, z-chunk 8
 
 
