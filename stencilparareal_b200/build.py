@@ -45,13 +45,18 @@ def build(force=False, verbose=False, checked=False):
     bdir = os.path.join(HERE, "_build_checked" if checked else "_build")
     os.makedirs(bdir, exist_ok=True)
     flags = NVCC_FLAGS + (["-DSP_BOUNDS_CHECK=1"] if checked else [])
+    # the translation units compile in parallel (one nvcc process each)
+    procs = []
     for src in SOURCES:
         obj = os.path.join(bdir, src.replace(".cu", ".o"))
         cmd = [nvcc()] + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+            print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib] + objs
     if verbose:
         print(" ".join(cmd))
