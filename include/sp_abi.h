@@ -270,8 +270,8 @@ long long sp_launch_count(void);
  * TMA/mbarrier pipeline).  op 9 and 10: the fused stage pairs 1+2 and 3+4 of
  * FP64 RK4 steps: tile rows, planes per CTA (0 = one range per resident CTA),
  * kind 2 when RK4 steps run as fused pairs (4: on 32-column tiles), else 0.
- * op 11: kind 3 when FP64 RK4
- * propagations run cluster-resident (sp_set_tune kind 3), else 0. */
+ * op 11: kind 3 when FP64 RK4 propagations run cluster-resident on z-slabs
+ * (sp_set_tune kind 3), 5 on (y,z) blocks (kind 5), else 0. */
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* kind);
 /* Runs the autotuner for this handle's grid at `batch` fields and precision: every
  * stage kernel gets the fastest of its candidate launch shapes, and FP64 RK4
@@ -283,7 +283,7 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
  * isolated timing, then compared, in the same sustained way, with both pairs
  * on their best 32 x 16 tiles, which are kept unless more than 1 % slower
  * (they move fewer DRAM bytes, so they hold a higher clock under the cap).
- * Small FP64 fields then take the cluster-resident path (kind 3 of
+ * Small FP64 fields then take a cluster-resident path (kind 3 or 5 of
  * sp_set_tune) when it is faster.  Takes about 1-3 s. */
 int sp_autotune(sp_convection* h, int precision, int batch);
 /* Test of the error path of the bounded in-kernel waits: runs one kernel whose
@@ -316,7 +316,12 @@ int sp_kernel_times(sp_convection* h, const double* field, double dt, int reps, 
  * kind 3 (FP64, small fields): every RK4 step of a DoRK4
  * call (or of a Parareal fine sweep) in one launch, each field held in the
  * shared memory of a thread-block cluster (ty and zchunk unused; needs an even
- * ni, at most 2048 cells per plane and nk = C x {2,3,4} with 2 <= C <= 16). */
+ * ni, at most 2048 cells per plane and nk = C x {2,3,4} with 2 <= C <= 16):
+ * CTA c of the cluster holds planes of the field (z-slabs).  kind 5 (FP64,
+ * small fields): the same with CTA (ry, rz) holding a block of nj/cy rows and
+ * nk/cz planes, cy, cz >= 2, cy x cz <= 16, each block at least 2 x 2: it sends
+ * a stage's boundary values to four neighbours, half as many values as the
+ * z-slabs at 32^3 on 16 CTAs. */
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind);
 
 #ifdef __cplusplus

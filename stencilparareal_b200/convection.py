@@ -187,7 +187,8 @@ class Convection:
         """kind: 0 direct loads, 1 TMA/mbarrier pipeline (single-stage kernels);
         2 fused stage pairs for FP64 RK4 steps on 64-column tiles (ty 8 or 16); 4 the
         same on 32 x 16 tiles (ty 16); 3 the cluster-resident path for FP64 RK4
-        propagations of small fields (ty and zchunk unused)."""
+        propagations of small fields, the field split into z-slabs, 5 the same
+        split into (y,z) blocks (ty and zchunk unused)."""
         L.check(L.lib().sp_set_tune(self._h, precision, batch, ty, zchunk, int(kind)))
 
     def autotune(self, precision: int = L.SP_F64, batch: int = 1):

@@ -47,7 +47,8 @@ struct Tune {
     Shape op[kNumOps];
     Shape pair[2] = {Shape{8, 0, 1}, Shape{8, 0, 1}};  // fused stage pairs 1+2 and 3+4 (ty 8 or 16)
     int fused = 0;    // 1: FP64 RK4 steps run as the two fused pairs
-    int cluster = 0;  // 1: FP64 RK4 propagations of small fields run cluster-resident (sp_cluster.cu)
+    int cluster = 0;  // FP64 RK4 propagations of small fields run cluster-resident (sp_cluster.cu):
+                      // 1 on z-slabs, 2 on (y,z) blocks
     void set_all(const Shape& s) {
         for (auto& o : op) o = s;
     }
@@ -109,8 +110,11 @@ struct ClusterLaunch {
     const void* wtab = nullptr;
     const int* item_lo = nullptr;    // as in StageLaunch
     int item_base = 0;
+    int mode = 1;                    // 1: z-slabs (k_rk4_cluster), 2: (y,z) blocks (k_rk4_cluster2d)
 };
-bool cluster_supported(const Geo& g);  // FP64, even ni, small planes, nk = C * {2,3,4} with 2 <= C <= 16
+// mode 1: FP64, even ni, small planes, nk = C * {2,3,4} with 2 <= C <= 16;
+// mode 2: FP64, even ni, nj = cy * BY, nk = cz * BZ with cy, cz, BY, BZ >= 2, cy * cz <= 16
+bool cluster_supported(const Geo& g, int mode = 1);
 cudaError_t prepare_cluster();
 cudaError_t launch_rk4_cluster(const Geo& g, const ClusterLaunch& L, cudaStream_t s, int* err);
 size_t cluster_weights_bytes();

@@ -396,10 +396,11 @@ int do_prop(sp_convection* h, int prec, bool rk, const void* in, void* out, doub
     // Periodicity on the input, in place, as before the reference's first stencil.
     SP_CUDA(launch_periodicity(g, const_cast<void*>(in), 1, s));
     const bool const_nu = h->P.nufreq == 0.;
-    if (rk && t.cluster && prec == 0 && cluster_supported(g) && (const_nu || !capturing(s))) {
+    if (rk && t.cluster && prec == 0 && cluster_supported(g, t.cluster) && (const_nu || !capturing(s))) {
         // small field: every step in one launch, the field held in a cluster's
         // shared memory (sp_cluster.cu); then the periodic images of `out`
         ClusterLaunch L;
+        L.mode = t.cluster;
         L.in = in;
         L.out = out;
         L.nsteps = n;
@@ -566,15 +567,19 @@ int sp_convection_synchronize(sp_convection* h) {
 
 int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, int kind) {
     if (!h || (precision != SP_F64 && precision != SP_F32) || batch < 1) return fail(SP_ERR_INVALID, "bad tune args");
-    if (kind < 0 || kind > 4)
-        return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA), 2 (fused pairs), 3 (cluster-resident) "
-                                    "or 4 (fused pairs on 32-column tiles)");
-    if (kind == 3) {
-        if (precision != SP_F64 || !cluster_supported(h->g[0]))
-            return fail(SP_ERR_INVALID, "the cluster-resident path needs FP64, an even ni, small planes and nk = C x "
-                                        "{2,3,4} with 2 <= C <= 16");
+    if (kind < 0 || kind > 5)
+        return fail(SP_ERR_INVALID, "kernel kind must be 0 (direct), 1 (TMA), 2 (fused pairs), 3 (cluster-resident "
+                                    "on z-slabs), 4 (fused pairs on 32-column tiles) or 5 (cluster-resident on (y,z) "
+                                    "blocks)");
+    if (kind == 3 || kind == 5) {
+        if (precision != SP_F64 || !cluster_supported(h->g[0], kind == 3 ? 1 : 2))
+            return fail(SP_ERR_INVALID, kind == 3 ? "the cluster-resident path on z-slabs needs FP64, an even ni, small "
+                                                    "planes and nk = C x {2,3,4} with 2 <= C <= 16"
+                                                  : "the cluster-resident path on (y,z) blocks needs FP64, an even ni "
+                                                    "and nj = cy x BY, nk = cz x BZ with cy, cz, BY, BZ >= 2, "
+                                                    "cy x cz <= 16, whose buffers fit in shared memory");
         Tune t = h->tune(precision, batch);
-        t.cluster = 1;
+        t.cluster = kind == 3 ? 1 : 2;
         h->tunes[{precision, batch}] = t;
         h->drop_graphs();
         return SP_OK;
@@ -612,8 +617,8 @@ int sp_set_tune(sp_convection* h, int precision, int batch, int ty, int zchunk, 
 
 // op 0..8: single-stage kernels (tma: 0 direct, 1 TMA); op 9, 10: fused pairs
 // 1+2 and 3+4 (tma: 2 when RK4 steps run fused, 4 when fused on 32-column
-// tiles, else 0); op 11: the
-// cluster-resident path (tma: 3 when FP64 RK4 propagations use it, else 0).
+// tiles, else 0); op 11: the cluster-resident path (tma: 3 when FP64 RK4
+// propagations use it on z-slabs, 5 on (y,z) blocks, else 0).
 int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty, int* zchunk, int* tma) {
     if (!h) return fail(SP_ERR_INVALID, "null handle");
     const Tune tn = h->tune(precision, batch);
@@ -624,7 +629,7 @@ int sp_tuned_config(sp_convection* h, int precision, int batch, int op, int* ty,
         kind = tn.fused ? (t.tx == 32 ? 4 : 2) : 0;
     } else if (op == kNumOps + 2) {
         t = Shape{0, 0, 0};
-        kind = tn.cluster ? 3 : 0;
+        kind = tn.cluster == 2 ? 5 : (tn.cluster ? 3 : 0);
     } else {
         t = tn.op[op < 0 || op >= kNumOps ? OP_RK_S2 : op];
         kind = t.tma;
@@ -1087,15 +1092,16 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
             }
         }
     }
-    // small fields: the cluster-resident path against the best of the above,
-    // timed as it is used (a DoRK4 of a graph chunk of steps for one field; four
-    // batched steps for a batch)
+    // small fields: the cluster-resident paths (z-slabs, (y,z) blocks) against
+    // the best of the above, timed as they are used (a DoRK4 of a graph chunk of
+    // steps for one field; four batched steps for a batch)
     best.cluster = 0;
-    if (precision == SP_F64 && cluster_supported(g)) {
+    if (precision == SP_F64 && (cluster_supported(g, 1) || cluster_supported(g, 2))) {
         int* err = h->err.as<int>();
-        float path_ms[2] = {1e30f, 1e30f};
+        float path_ms[3] = {1e30f, 1e30f, 1e30f};
         SP_CUDA(fill_wave(p, 5 * fb, g.es, s));
-        for (int c = 0; c < 2 && rc == SP_OK; ++c) {
+        for (int c = 0; c < 3 && rc == SP_OK; ++c) {
+            if (c && !cluster_supported(g, c)) continue;
             Tune tt = best;
             tt.cluster = c;
             h->tunes[{precision, batch}] = tt;
@@ -1106,6 +1112,7 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 cudaError_t x = cudaSuccess;
                 if (c) {
                     ClusterLaunch L;
+                    L.mode = c;
                     L.in = p; L.out = p; L.items = batch; L.nsteps = 4; L.dt = dtt; L.nu = nu; L.coef = h->coef;
                     x = launch_rk4_cluster(g, L, s, err);
                 } else {
@@ -1125,14 +1132,15 @@ extern "C" int sp_autotune(sp_convection* h, int precision, int batch) {
                 cudaEventElapsedTime(&m, e0, e1);
                 path_ms[c] = std::min(path_ms[c], m);
             }
+            if (rc != SP_OK && c) {
+                // a cluster launch can be refused (cluster shape not schedulable): keep the other paths
+                cudaGetLastError();
+                rc = SP_OK;
+                path_ms[c] = 1e30f;
+            }
         }
-        if (rc != SP_OK) {
-            // the cluster launch can be refused (cluster shape not schedulable): keep the other path
-            cudaGetLastError();
-            rc = SP_OK;
-            path_ms[1] = 1e30f;
-        }
-        best.cluster = path_ms[1] < path_ms[0] ? 1 : 0;
+        for (int c = 1; c < 3; ++c)
+            if (path_ms[c] < path_ms[best.cluster]) best.cluster = c;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1355,7 +1363,8 @@ int enqueue_coarse(sp_parareal* pr, const void* src, const Geo& gsrc, double t0,
 // (small fields), fused stage pairs, or the four stage kernels per step.
 bool cluster_sweep(const sp_parareal* pr) {
     sp_convection* h = pr->prop;
-    return h->P.nufreq == 0. && h->tune(0, pr->P).cluster && cluster_supported(pr->g64);
+    const int mode = h->tune(0, pr->P).cluster;
+    return h->P.nufreq == 0. && mode && cluster_supported(pr->g64, mode);
 }
 bool fused_sweep(const sp_parareal* pr) {
     sp_convection* h = pr->prop;
@@ -1404,6 +1413,7 @@ int emit_iteration(sp_parareal* pr, cudaStream_t s, bool events, int parts, int 
     if (cluster && (parts & 1) && e == cudaSuccess) {
         // every fine step of every iterating slice in one launch, each slice in one cluster
         ClusterLaunch L;
+        L.mode = tf.cluster;
         L.in = pr->u(0);
         L.out = pr->f(0);
         L.items = P;
