@@ -220,8 +220,9 @@ def cpu_vs_gpu_times(torch, sp, device, gpu_serial_128_s=None):
     out["serial_fine_32cube_1000_steps"] = {"what": "32^3, 1000 RK4 FP64 steps, dt=1e-4, c=(1,1,1), nu=0.01",
                                             "cpu_s": cpu, "gpu_s": gpu["autotuned"],
                                             "gpu_s_stage_kernels": gpu["stage_kernels"],
-                                            "gpu_path": "cluster-resident" if tuned["cluster"]["kind"] == 3
-                                            else "stage kernels / fused pairs"}
+                                            "gpu_path": {3: "cluster-resident on z-slabs",
+                                                         5: "cluster-resident on (y,z) blocks"}.get(
+                                                tuned["cluster"]["kind"], "stage kernels / fused pairs")}
     n, sample, total = 128, 200, 20000
     p = O.params(n, nu0=0.01, cx=1.0, cy=1.0, cz=1.0)
     q0 = gaussian_noise(n, seed=0)
@@ -322,7 +323,7 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
             a64 = conv.autotune(sp.SP_F64, 16)
             # the cluster-resident path or the fused stage pairs when the tuner
             # preferred them, else the stage kernels' shape
-            t64 = (a64["cluster"] if a64["cluster"]["kind"] == 3 else
+            t64 = (a64["cluster"] if a64["cluster"]["kind"] in (3, 5) else
                    a64["P12"] if a64["P12"]["kind"] in (2, 4) else a64["S2"])
             tunes[n] = (t64, conv.autotune(sp.SP_F32, 1)["S2"])
         t64, t32 = tunes[n]

@@ -90,7 +90,7 @@ def _run_pinned_parareal(sp, name, tune_like_batch):
     if tune_like_batch:
         # the batch benchmark's tuning: the batched tune of 16 fields applied to P
         a64 = conv.autotune(sp.SP_F64, 16)
-        t64 = (a64["cluster"] if a64["cluster"]["kind"] == 3 else
+        t64 = (a64["cluster"] if a64["cluster"]["kind"] in (3, 5) else
                a64["P12"] if a64["P12"]["kind"] in (2, 4) else a64["S2"])
         t32 = conv.autotune(sp.SP_F32, 1)["S2"]
         conv.set_tune(sp.SP_F64, P, t64["ty"], t64["zchunk"], t64["kind"])
