@@ -18,6 +18,12 @@ region.
 (oracle/, the reference itself needs Boost and MPI and cannot be built here)
 on the host cores on a bounded sample of the same workload.
 
+At N=1 the line also carries the one-GPU Parareal (`parareal`), the batch of
+uneven instances (`batch`), the adjoint (`adjoint`) and `paper`: the
+reference's own published GPU experiment (128^3, 32768 RK4 steps; Parareal
+with 128 slices and 3 iterations) timed on this GPU beside its published
+times, the only workload of this path with published numbers.
+
 Launch: python bench.py [--gpus N --steps K --warmup W]; N>1 under torchrun.
 The headline value at N>1 is N independent replicas of the fine-propagator
 step (the propagator does not shard: "weak" scaling with no collective on
@@ -296,6 +302,49 @@ def parareal_summary(torch, sp, device):
     return out
 
 
+def paper_summary(torch, sp, device, P=128, kmax=3):
+    """The reference's published GPU experiment, timed on this one GPU: 128^3,
+    T=0.1, nu0=0.1, nufreq=0, c=(1,1,1), fine RK4 FP64 with 32768 steps, coarse
+    upwind Euler FP64 with 2048 steps, the analytic field exactQ at t=0, no
+    asynchronous first step, kmax=3 iterations without a tolerance
+    (jobs/paperJobs/04-SpeedupGPU.job:42-48, 01-Convergence.job:51-57), P=128
+    slices -- there one GPU per slice, here all slices on this GPU.  Published
+    the serial fine run took 191.0-191.1 s on one sm_35
+    GPU (03-ReferenceGPU/run_4.log:24) and 896.7-912.0 s on 8 CPU threads
+    (02-SpeedupThreads), Parareal with 128 slices 7.28 s on 128 GPUs
+    (04-SpeedupGPU/runtime.dat:6), error after 3 iterations 1.73145e-07
+    (01-Convergence/result.dat:5)."""
+    from stencilparareal_b200.solution import fill_q
+    n, nu0, T, tsF, tsC = 128, 0.1, 0.1, 32768, 2048
+    conv = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, 1.0, 1.0, 1.0, device=device)
+    conv.autotune(sp.SP_F64, 1)
+    conv.autotune(sp.SP_F64, P)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, gridSize=n, endTime=T, timeStepsFine=tsF,
+                                   timeStepsCoarse=tsC, kmax=kmax)
+    q0, qs, q = conv.field(), conv.field(), conv.field()
+    conv.upload(q0, fill_q(n, n, n, nu0, 0.0, 1.0, 1.0, 1.0, 0.0))
+    ser = sp.Parareal(conv, q0, qs, 0.0, conf, coarse="euler", coarse_precision="f64")
+    conv.synchronize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ser.DoSerial()
+    conv.synchronize()
+    t_serial = time.perf_counter() - t0
+    par = sp.Parareal(conv, q0, q, 0.0, conf, coarse="euler", coarse_precision="f64")
+    par.DoParallel(reference=qs)  # warm (graph capture)
+    rep = par.DoParallel(reference=qs)
+    pub_serial, pub_par = 191.0, 7.28
+    return {"config": "reference paper experiment: 128^3, T=0.1, nu0=0.1, nufreq=0, c=(1,1,1), fine RK4 FP64 32768 "
+                      "steps, coarse upwind Euler FP64 2048 steps, exactQ IC, kmax=3, P=128 slices on 1 GPU",
+            "serial_fine_s": t_serial, "serial_fine_gcups": n ** 3 * tsF / t_serial / 1e9,
+            "published_serial_fine_gpu_s": pub_serial, "published_serial_fine_cpu8_s": [896.7, 912.0],
+            "serial_speedup_vs_published_gpu": pub_serial / t_serial,
+            "parareal_s": rep["seconds"], "iterations": rep["iterations"],
+            "err_max_vs_serial": rep["err_max"], "published_err_max_k3": 1.73145e-07,
+            "published_parareal_128_gpus_s": pub_par, "parareal_1gpu_vs_published_128_gpus": pub_par / rep["seconds"],
+            "speedup_vs_serial_same_gpu": t_serial / rep["seconds"]}
+
+
 def batch_summary(torch, sp, device, n_inst=48, seed=2):
     """Batched uneven instances: 48 independent Parareal solves, grids drawn from {32,48,64,96}^3, nu log-uniform in
     [1e-4, 1e-2], c uniform in [-1,1]^3, 8-24 slices; T=0.05, fine RK4 FP64 dt=1e-5, coarse RK4 FP32
@@ -477,6 +526,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-parareal", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-paper", action="store_true", help="skip the reference's published experiment (128^3, "
+                                                            "32768 RK4 steps; Parareal P=128, kmax=3)")
     ap.add_argument("--tune", default="auto", help="'auto' or ty,zchunk,kind for the stage kernels")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: one DoRK4 of --profile-steps steps on the 256^3 workload (or a "
@@ -679,6 +730,11 @@ def main():
                     line[key] = fn(torch, sp, device)
                 except Exception as ex:  # reported, not hidden
                     line[key] = {"error": repr(ex)}
+        if not args.no_paper:
+            try:
+                line["paper"] = paper_summary(torch, sp, device)
+            except Exception as ex:  # reported, not hidden
+                line["paper"] = {"error": repr(ex)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample()
             try:
