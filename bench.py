@@ -309,7 +309,7 @@ def paper_summary(torch, sp, device, P=128, kmax=3):
     asynchronous first step, kmax=3 iterations without a tolerance
     (jobs/paperJobs/04-SpeedupGPU.job:42-48, 01-Convergence.job:51-57), P=128
     slices -- there one GPU per slice, here all slices on this GPU.  Published
-    the serial fine run took 191.0-191.1 s on one sm_35
+    by the reference's job logs: the serial fine run took 191.0-191.1 s on one sm_35
     GPU (03-ReferenceGPU/run_4.log:24) and 896.7-912.0 s on 8 CPU threads
     (02-SpeedupThreads), Parareal with 128 slices 7.28 s on 128 GPUs
     (04-SpeedupGPU/runtime.dat:6), error after 3 iterations 1.73145e-07
