@@ -423,71 +423,98 @@ def batch_summary(torch, sp, device, n_inst=48, seed=2):
     return out
 
 
-def pipeline_summary(torch, sp, dist, rank, world, device, n=128, P=32):
+def pipeline_summary(torch, sp, dist, rank, world, device, n=128, P=32, problem="config3"):
     """The Parareal slice pipeline over the ranks of the process group (one GPU
-    each): the one-GPU Parareal workload (n^3, P slices, T=0.2, fine RK4 FP64
-    dt=1e-5, coarse RK4 FP32, increment form), rank r holding the slice window
-    slice_bounds(P, world, r); per iteration every rank runs its batched fine
-    sweep, receives the previous rank's boundary field (NCCL recv into its own
-    HBM), runs its coarse sweep and corrections and sends its boundary field on
-    (the reference's MPI ring, Parareal.h:116-165), stopping once the defect
-    over all ranks is below 1e-8.  Time: CUDA events on each rank's library
-    stream, max over ranks.  Rank 0 also times the same problem on its GPU
-    alone (DoParallel, same stopping rule) for comparison."""
+    each), rank r holding the slice window slice_bounds(P, world, r); per
+    iteration every rank runs its batched fine sweep, receives the previous
+    rank's boundary field (NCCL recv into its own HBM), runs its coarse sweep
+    and corrections and sends its boundary field on (the reference's MPI ring,
+    Parareal.h:116-165).  Time: CUDA events on each rank's library stream, max
+    over ranks.  Rank 0 also times the same problem on its GPU alone
+    (DoParallel, same stopping rule) for comparison.
+
+    problem "config3": the one-GPU Parareal workload (n^3, P slices, T=0.2, fine
+    RK4 FP64 dt=1e-5, coarse RK4 FP32, increment form), stopping once the
+    defect over all ranks is below 1e-8.  problem "paper": the reference's
+    published GPU experiment (n^3, T=0.1, nu0=0.1, 32768 fine RK4 and 2048
+    coarse upwind-Euler FP64 steps, exactQ initial field, 3 iterations, no
+    tolerance; jobs/paperJobs/04-SpeedupGPU.job:42-48), whose 128-slice run
+    took 7.28 s on 128 GPUs (04-SpeedupGPU/runtime.dat:6)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ics import gaussian_noise
     from stencilparareal_b200.parareal import DistributedParareal, WindowParareal, slice_bounds
-    T, tsF, tsC, tol = 0.2, 20000, 200, 1e-8
-    conv = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+    from stencilparareal_b200.solution import fill_q
+    paper = problem == "paper"
+    if paper:
+        nu0, T, tsF, tsC, kmax, tol = 0.1, 0.1, 32768, 2048, 3, 0.0
+        coarse = dict(coarse="euler", coarse_precision="f64")
+    else:
+        nu0, T, tsF, tsC, kmax, tol = 0.01, 0.2, 20000, 200, 8, 1e-8
+        coarse = dict(coarse="rk4", coarse_precision="f32")
+    conv = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, 1.0, 1.0, 1.0, device=device)
     lo, hi = slice_bounds(P, world, rank)
     conv.autotune(sp.SP_F64, 1)
     conv.autotune(sp.SP_F64, hi - lo)
-    conv.autotune(sp.SP_F32, 1)
-    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=0.01, gridSize=n, endTime=T, timeStepsFine=tsF,
-                                   timeStepsCoarse=tsC, kmax=8)
+    if not paper:
+        conv.autotune(sp.SP_F32, 1)
+    conf = sp.RuntimeConfiguration(timeSlices=P, nu0=nu0, gridSize=n, endTime=T, timeStepsFine=tsF,
+                                   timeStepsCoarse=tsC, kmax=kmax)
+    q_init = fill_q(n, n, n, nu0, 0.0, 1.0, 1.0, 1.0, 0.0) if paper else gaussian_noise(n, seed=0)
     f0, fs, fref = conv.field(), conv.field(), conv.field()
-    conv.upload(f0, gaussian_noise(n, seed=0))
+    conv.upload(f0, q_init)
     last = rank == world - 1
     if last:  # the serial fine solution, for the error of the result
-        sp.Parareal(conv, f0, fref, 0.0, conf).DoSerial()
-    w = WindowParareal(conv, f0, fs, 0.0, conf, lo, hi - lo, coarse="rk4", coarse_precision="f32")
+        sp.Parareal(conv, f0, fref, 0.0, conf, **coarse).DoSerial()
+    w = WindowParareal(conv, f0, fs, 0.0, conf, lo, hi - lo, **coarse)
     dp = DistributedParareal(w)
-    dp.run(8, tol)  # warm: graph capture, communicator set-up
+    dp.run(kmax, tol)  # warm: graph capture, communicator set-up
     conv.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(conv.stream)
-    its, defects = dp.run(8, tol)
+    its, defects = dp.run(kmax, tol)
     e1.record(conv.stream)
     conv.synchronize()
     torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) * 1e-3
-    err = conv.errors(w.boundary, fref)[1] if last else 0.0
-    t = torch.tensor([secs, err], dtype=torch.float64, device=f"cuda:{device}" if dist.get_backend() == "nccl"
-                     else "cpu")
+    err_max, err_l2 = conv.errors(w.boundary, fref) if last else (0.0, 0.0)
+    t = torch.tensor([secs, err_max, err_l2], dtype=torch.float64,
+                     device=f"cuda:{device}" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    secs_max, err_last = float(t[0]), float(t[1])
+    secs_max, err_max, err_l2 = float(t[0]), float(t[1]), float(t[2])
     one_gpu_s = None
     if rank == 0:
         # the same problem on this GPU alone, for comparison
-        c1 = sp.Convection(n, n, n, 1.0 / n, 0.01, 0.0, 1.0, 1.0, 1.0, device=device)
+        c1 = sp.Convection(n, n, n, 1.0 / n, nu0, 0.0, 1.0, 1.0, 1.0, device=device)
         c1.autotune(sp.SP_F64, P)
-        c1.autotune(sp.SP_F32, 1)
+        if not paper:
+            c1.autotune(sp.SP_F32, 1)
         g0, g1 = c1.field(), c1.field()
-        c1.upload(g0, gaussian_noise(n, seed=0))
-        par = sp.Parareal(c1, g0, g1, 0.0, conf, coarse="rk4", coarse_precision="f32", tol=tol, tol_kind="defect")
+        c1.upload(g0, q_init)
+        stop = {} if paper else dict(tol=tol, tol_kind="defect")
+        par = sp.Parareal(c1, g0, g1, 0.0, conf, **coarse, **stop)
         par.DoParallel()
         one_gpu_s = par.DoParallel()["seconds"]
     dist.barrier()
-    return {"config": f"{n}^3, P={P}, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (200 rounded up to a multiple "
-                      f"of P), increment form, Gaussian+noise IC seed 0, c=(1,1,1), nu=0.01; slice windows "
-                      f"{[slice_bounds(P, world, r) for r in range(world)]}",
-            "ranks": world, "exchange": f"torch.distributed {dist.get_backend()} send/recv of one FP64 field "
-                                        f"per iteration and rank boundary, MAX all-reduce of the defect",
-            "stop_rule": "defect < 1e-8 (max over ranks)", "iterations": its, "defects": defects,
-            "seconds": secs_max, "err_l2_vs_serial": err_last, "one_gpu_parareal_s": one_gpu_s,
-            "speedup_vs_one_gpu": one_gpu_s / secs_max if one_gpu_s else None}
+    if paper:
+        cfg = (f"reference paper experiment: {n}^3, P={P}, T=0.1, nu0=0.1, c=(1,1,1), fine RK4 FP64 32768 steps, "
+               f"coarse upwind Euler FP64 2048 steps (rounded up to a multiple of P), exactQ IC, 3 iterations")
+        stop_rule = "fixed 3 iterations (kmax=3, no tolerance), as the reference's job"
+    else:
+        cfg = (f"{n}^3, P={P}, T=0.2, fine RK4 FP64 dt=1e-5, coarse RK4 FP32 (200 rounded up to a multiple "
+               f"of P), increment form, Gaussian+noise IC seed 0, c=(1,1,1), nu=0.01")
+        stop_rule = "defect < 1e-8 (max over ranks)"
+    out = {"config": cfg + f"; slice windows {[slice_bounds(P, world, r) for r in range(world)]}",
+           "ranks": world, "exchange": f"torch.distributed {dist.get_backend()} send/recv of one FP64 field "
+                                       f"per iteration and rank boundary, MAX all-reduce of the defect",
+           "stop_rule": stop_rule, "iterations": its, "defects": defects,
+           "seconds": secs_max, "err_l2_vs_serial": err_l2, "err_max_vs_serial": err_max,
+           "one_gpu_parareal_s": one_gpu_s,
+           "speedup_vs_one_gpu": one_gpu_s / secs_max if one_gpu_s else None}
+    if paper and n == 128 and P == 128:
+        out["published_parareal_128_gpus_s"] = 7.28
+    return out
 
 
 def adjoint_summary(torch, sp, device):
@@ -541,6 +568,9 @@ def main():
                     help="N>1: run only the Parareal slice pipeline (prints its JSON object)")
     ap.add_argument("--pipeline-grid", type=int, default=128)
     ap.add_argument("--pipeline-slices", type=int, default=32)
+    ap.add_argument("--pipeline-problem", default="config3", choices=["config3", "paper"],
+                    help="N>1: the slice pipeline's problem: the one-GPU Parareal workload (128^3, P=32, defect "
+                         "rule) or the reference's published experiment (use --pipeline-slices 128)")
     ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
                     help="process-group backend for N>1 (gloo: exchange through host memory)")
     args = ap.parse_args()
@@ -564,7 +594,8 @@ def main():
         kw = {"device_id": torch.device(f"cuda:{device}")} if args.dist_backend == "nccl" else {}
         dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120), **kw)
         if args.pipeline_only:
-            out = pipeline_summary(torch, sp, dist, rank, world, device, args.pipeline_grid, args.pipeline_slices)
+            out = pipeline_summary(torch, sp, dist, rank, world, device, args.pipeline_grid, args.pipeline_slices,
+                                   args.pipeline_problem)
             if rank == 0:
                 print(json.dumps({"parareal_pipeline": out}), flush=True)
             dist.barrier()
@@ -745,7 +776,7 @@ def main():
     if dist and not args.no_pipeline:
         # every rank takes part: the Parareal slice pipeline over the process group
         line["parareal_pipeline"] = pipeline_summary(torch, sp, dist, rank, world, device, args.pipeline_grid,
-                                                     args.pipeline_slices)
+                                                     args.pipeline_slices, args.pipeline_problem)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

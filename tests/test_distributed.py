@@ -117,22 +117,34 @@ def test_two_processes_one_gpu_equal_single_process(sp, orc, coarse, prec):
 
 
 @pytest.mark.gpu
-def test_benchmark_slice_pipeline_two_ranks_one_gpu(sp):
+@pytest.mark.parametrize("problem", ["config3", "paper"])
+def test_benchmark_slice_pipeline_two_ranks_one_gpu(sp, problem):
     """bench.py's N>1 Parareal slice pipeline, launched as the benchmark is (torchrun,
     one process per rank), with the gloo backend so that both ranks can share the
     one GPU here (the exchange goes through host memory; no kernel waits on the
-    other process).  On N GPUs the same code exchanges over NCCL."""
+    other process).  On N GPUs the same code exchanges over NCCL.  Both problems:
+    the one-GPU Parareal workload (defect rule) and the reference's published
+    experiment (Euler coarse, exactQ, 3 fixed iterations), on a 16^3 grid."""
     import json
     import subprocess
     import sys
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"), "--gpus", "2",
-           "--pipeline-only", "--dist-backend", "gloo", "--pipeline-grid", "16", "--pipeline-slices", "6"]
+           "--pipeline-only", "--dist-backend", "gloo", "--pipeline-grid", "16", "--pipeline-slices", "6",
+           "--pipeline-problem", problem]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-3000:]
     line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
     out = json.loads(line)["parareal_pipeline"]
     assert out["ranks"] == 2
-    assert 1 <= out["iterations"] <= 6 and out["defects"][-1] < 1e-8
-    assert out["err_l2_vs_serial"] < 1e-8
+    if problem == "config3":
+        assert 1 <= out["iterations"] <= 6 and out["defects"][-1] < 1e-8
+        assert out["err_l2_vs_serial"] < 1e-8
+    else:
+        # three iterations of 6 slices: the result approaches the serial fine run
+        # (at 128^3 the reference's table has 1e-3, 1e-5, 1e-7; the upwind Euler
+        # coarse propagator is less accurate on 16^3: 1.4e-4 after 3 iterations)
+        assert out["iterations"] == 3
+        assert 0 < out["err_max_vs_serial"] < 1e-3
+        assert out["defects"][0] > out["defects"][1] > out["defects"][2]
     assert out["seconds"] > 0 and out["one_gpu_parareal_s"] > 0
