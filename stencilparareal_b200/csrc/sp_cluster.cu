@@ -299,8 +299,11 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster(const __grid
 // Arithmetic, buffers, barriers and the early sends as in k_rk4_cluster; a
 // halo region is read only by threads that send to the neighbour writing it,
 // and they send after all their reads, so two buffers suffice here too.
-template <int ZT, int UPT>
-__global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster2d(const __grid_constant__ ClusterArgs a) {
+// NT threads per CTA: 256 (up to 255 registers, one unit per thread) where the
+// block's units fit, else 512 (128 registers, up to two units per thread); at
+// 32^3 and 24^3 the 256-thread form is ~14 % faster, at 40^3 it would spill.
+template <int ZT, int UPT, int NT>
+__global__ void __launch_bounds__(NT, 1) k_rk4_cluster2d(const __grid_constant__ ClusterArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // 2 mbarriers (stage parity)
     double* buf = reinterpret_cast<double*>(smem_raw + 16);
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster2d(const __gr
     bool halo[UPT];                       // the unit's star reaches a halo row or plane
 #pragma unroll
     for (int j = 0; j < UPT; ++j) {
-        const int u = tid + j * kClusterThreads;
+        const int u = tid + j * NT;
         uv[j] = u < units;
         const int uu = uv[j] ? u : 0;
         ux[j] = 2 * (uu % half);
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_rk4_cluster2d(const __gr
     {
         const int rows = BY + 4;
         const int n = (BZ + 4) * rows * half;
-        for (int i = tid; i < n; i += kClusterThreads) {
+        for (int i = tid; i < n; i += NT) {
             const int p = i / (rows * half);
             const int r = i - p * rows * half;
             const int yy = r / half;
@@ -562,7 +565,7 @@ size_t cluster2d_smem(int ni, int by, int bz) {
 }
 
 struct Blocks2d {
-    int cy = 0, cz = 0, zt = 0, upt = 0;
+    int cy = 0, cz = 0, zt = 0, upt = 0, nt = 0;
 };
 Blocks2d blocks_2d(const Geo& g, int items) {
     Blocks2d best;
@@ -574,28 +577,41 @@ Blocks2d blocks_2d(const Geo& g, int items) {
             const int by = g.nj / cy, bz = g.nk / cz;
             if (by < 2 || bz < 2) continue;
             if (cluster2d_smem(g.ni, by, bz) > (size_t)kClusterSmemMax) continue;
-            const int zt = bz % 2 == 0 ? 2 : 1;
-            const long long units = (long long)(g.ni / 2) * by * (bz / zt);
-            const int upt = (int)((units + kClusterThreads - 1) / kClusterThreads);
-            if (upt > 2) continue;
+            // 256 threads with one unit each, of the fewest planes ZT in {1, 2, 4}
+            // that fits (the most threads with work), else 512 threads with up
+            // to two units of ZT = 2 or 1 planes
+            int zt = 0, upt = 0, nt = 0;
+            for (int z : {1, 2, 4})
+                if (!zt && bz % z == 0 && (long long)(g.ni / 2) * by * (bz / z) <= 256) {
+                    zt = z;
+                    upt = 1;
+                    nt = 256;
+                }
+            if (!zt) {
+                zt = bz % 2 == 0 ? 2 : 1;
+                const long long units = (long long)(g.ni / 2) * by * (bz / zt);
+                upt = (int)((units + kClusterThreads - 1) / kClusterThreads);
+                nt = kClusterThreads;
+                if (upt > 2) continue;
+            }
             const long long ctas = (long long)items * cy * cz;
             const long long waves = (ctas + 147) / 148;
             const double cost = (double)waves * ((double)g.ni * by * bz + 0.5 * (4.0 * by + 4.0 * bz) * g.ni);
             if (!best.cy || cost < best_cost || (cost == best_cost && upt < best.upt)) {
-                best = Blocks2d{cy, cz, zt, upt};
+                best = Blocks2d{cy, cz, zt, upt, nt};
                 best_cost = cost;
             }
         }
     return best;
 }
 
-template <int ZT, int UPT>
+template <int ZT, int UPT, int NT>
 cudaError_t launch_one2d(const Geo& g, const Blocks2d& b, const ClusterArgs& a, int items, cudaStream_t s) {
-    auto k = k_rk4_cluster2d<ZT, UPT>;
+    auto k = k_rk4_cluster2d<ZT, UPT, NT>;
     const int C = b.cy * b.cz;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)(C * items));
-    cfg.blockDim = dim3(kClusterThreads);
+    cfg.blockDim = dim3(NT);
     cfg.dynamicSmemBytes = cluster2d_smem(g.ni, g.nj / b.cy, g.nk / b.cz);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -608,10 +624,10 @@ cudaError_t launch_one2d(const Geo& g, const Blocks2d& b, const ClusterArgs& a, 
     return cudaLaunchKernelEx(&cfg, k, a);
 }
 
-template <int ZT, int UPT>
+template <int ZT, int UPT, int NT>
 cudaError_t set_attr_cluster2d() {
     cudaError_t e = cudaSuccess;
-    auto k = k_rk4_cluster2d<ZT, UPT>;
+    auto k = k_rk4_cluster2d<ZT, UPT, NT>;
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmemMax);
     return e;
@@ -629,8 +645,10 @@ cudaError_t prepare_cluster() {
     chk(set_attr_cluster<2, 1>(nullptr)); chk(set_attr_cluster<2, 2>(nullptr));
     chk(set_attr_cluster<3, 1>(nullptr)); chk(set_attr_cluster<3, 2>(nullptr));
     chk(set_attr_cluster<4, 1>(nullptr)); chk(set_attr_cluster<4, 2>(nullptr));
-    chk(set_attr_cluster2d<1, 1>()); chk(set_attr_cluster2d<1, 2>());
-    chk(set_attr_cluster2d<2, 1>()); chk(set_attr_cluster2d<2, 2>());
+    chk(set_attr_cluster2d<1, 1, 512>()); chk(set_attr_cluster2d<1, 2, 512>());
+    chk(set_attr_cluster2d<2, 1, 512>()); chk(set_attr_cluster2d<2, 2, 512>());
+    chk(set_attr_cluster2d<1, 1, 256>()); chk(set_attr_cluster2d<2, 1, 256>());
+    chk(set_attr_cluster2d<4, 1, 256>());
     return e;
 }
 
@@ -661,11 +679,16 @@ cudaError_t launch_rk4_cluster(const Geo& g, const ClusterLaunch& L, cudaStream_
     a.cz = b2.cz;
     if (L.mode == 2) {
         add_launches(1);
+        if (b2.nt == 256) {
+            if (b2.zt == 4) return launch_one2d<4, 1, 256>(g, b2, a, L.items, s);
+            if (b2.zt == 2) return launch_one2d<2, 1, 256>(g, b2, a, L.items, s);
+            return launch_one2d<1, 1, 256>(g, b2, a, L.items, s);
+        }
         switch (b2.zt * 2 + b2.upt - 1) {
-            case 2: return launch_one2d<1, 1>(g, b2, a, L.items, s);
-            case 3: return launch_one2d<1, 2>(g, b2, a, L.items, s);
-            case 4: return launch_one2d<2, 1>(g, b2, a, L.items, s);
-            default: return launch_one2d<2, 2>(g, b2, a, L.items, s);
+            case 2: return launch_one2d<1, 1, 512>(g, b2, a, L.items, s);
+            case 3: return launch_one2d<1, 2, 512>(g, b2, a, L.items, s);
+            case 4: return launch_one2d<2, 1, 512>(g, b2, a, L.items, s);
+            default: return launch_one2d<2, 2, 512>(g, b2, a, L.items, s);
         }
     }
     const bool two = (long long)(g.ni / 2) * g.nj > kClusterThreads;

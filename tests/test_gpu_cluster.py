@@ -12,10 +12,11 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
 # grids: planes per CTA NZ = 2, 3, 4 (z-slabs), blocks of 2 .. 16 rows and planes
-# with one or two planes per unit ((y,z) blocks), clusters of 2 .. 16 CTAs, one
-# or two cell pairs per thread, non-cubic and non-power-of-two extents
+# with 1, 2 or 4 planes per unit and 256 or 512 threads ((y,z) blocks), clusters
+# of 2 .. 16 CTAs, one or two cell pairs per thread, non-cubic and
+# non-power-of-two extents
 SIZES = [(32, 32, 32), (24, 20, 12), (64, 32, 16), (16, 16, 8), (10, 6, 4), (30, 30, 9), (32, 32, 48),
-         (8, 12, 36), (40, 40, 32)]
+         (8, 12, 36), (40, 40, 32), (24, 24, 24)]
 
 
 def _conv(sp, n, nufreq=0.0, c=(1.0, -0.5, 0.25), nu0=0.02):
