@@ -22,6 +22,11 @@
 // after all its reads (its values depend on them).  Nothing goes to global
 // memory between the first load and the last store.
 //
+// k_rk4_cluster2d splits the field into (y,z) blocks instead of z-slabs: four
+// neighbours per CTA and, for the same number of CTAs, fewer halo values per
+// stage (half as many at 32^3 on 16 CTAs), which is what bounds the slabs.
+// The tuner times both layouts (tune kinds 3 and 5) and keeps the faster.
+//
 // Every value is computed with the operations, and in the order, of the
 // single-stage kernels (rhs_w13 and the 13-access low-storage epilogues of
 // sp_kernels.cu), so the result equals theirs bit for bit:
