@@ -305,13 +305,14 @@ class DistributedParareal:
             inbound = None
             if self.rank > 0:
                 buf = self._payload(recv_field)
-                dist.recv(buf, src=self.rank - 1, group=self.group, tag=k)
+                # NCCL has no tags (messages between two ranks arrive in order)
+                dist.recv(buf, src=self.rank - 1, group=self.group, tag=k if self.gloo else 0)
                 if buf is not (recv_field.data if hasattr(recv_field, "data") else recv_field):
                     (recv_field.data if hasattr(recv_field, "data") else recv_field).copy_(buf)
                 inbound = recv_field
             d = w.coarse(k, inbound)
             if self.rank < self.world - 1:
-                dist.send(self._payload(w.boundary), dst=self.rank + 1, group=self.group, tag=k)
+                dist.send(self._payload(w.boundary), dst=self.rank + 1, group=self.group, tag=k if self.gloo else 0)
             t = torch.tensor([d], dtype=torch.float64)
             if not self.gloo:
                 t = t.cuda()
