@@ -557,12 +557,12 @@ cudaError_t launch_one(const Geo& g, const ClusterArgs& a, int items, cudaStream
 }
 
 // (y,z) blocks for a grid and batch: cy, cz >= 2 with C = cy * cz <= 16, blocks
-// of at least 2 rows and 2 planes whose two buffers fit, ZT = 2 planes per unit
-// when BZ is even (else 1) and at most 2 units per thread.  Among those the one
-// with the least estimated time: waves of CTAs (one per SM) x (own cells + half
-// the halo cells per CTA; at 32^3 the exchange of a halo cell costs about half
-// the stage work of an own cell); ties go to fewer units per thread.  cy = 0
-// when the grid has no such blocks.
+// of at least 2 rows and 2 planes whose two buffers fit, and a thread form
+// (below).  Among those the one with the least estimated time: waves of CTAs
+// (one per SM) x (own cells + half the halo cells per CTA; at 32^3 the exchange
+// of a halo cell costs about half the stage work of an own cell), x 1.6 for the
+// spilling two-unit form; ties go to fewer units per thread.  cy = 0 when the
+// grid has no such blocks.
 // bytes of shared memory per CTA of k_rk4_cluster2d: barriers, two buffers of
 // the block with its halo rows and planes, the accumulator of the own cells
 size_t cluster2d_smem(int ni, int by, int bz) {
@@ -601,7 +601,12 @@ Blocks2d blocks_2d(const Geo& g, int items) {
             }
             const long long ctas = (long long)items * cy * cz;
             const long long waves = (ctas + 147) / 148;
-            const double cost = (double)waves * ((double)g.ni * by * bz + 0.5 * (4.0 * by + 4.0 * bz) * g.ni);
+            // the 512-thread form with two units per thread spills at its
+            // 128-register cap: a batch of 16 fields of 32^3 ran its fine sweep
+            // at 22.6 GCUPS on (2,4) blocks in one wave of that form, at 40.8 on
+            // (4,4) blocks in two waves of the 256-thread form
+            const double form = nt == kClusterThreads && upt == 2 ? 1.6 : 1.0;
+            const double cost = form * (double)waves * ((double)g.ni * by * bz + 0.5 * (4.0 * by + 4.0 * bz) * g.ni);
             if (!best.cy || cost < best_cost || (cost == best_cost && upt < best.upt)) {
                 best = Blocks2d{cy, cz, zt, upt, nt};
                 best_cost = cost;
