@@ -82,6 +82,19 @@ def test_cluster_path_time_dependent_nu_in_place_and_long_runs(sp, orc, kind):
     assert rel_l2(c, orc.rk4(orc.params(32, nu0=0.01), q1, 0.0, 1e-4, 1000)) < TOL64
 
 
+def test_blocks_with_two_units_per_thread_time_dependent_nu_in_place(sp, orc):
+    """(y,z) blocks in the 512-thread form with two units per thread (40^3: 4 x 4
+    blocks of 10 rows and 8 planes), with per-step weights (nu(t)) and in place."""
+    n = (40, 40, 32)
+    conv = _conv(sp, n, nufreq=60.0)
+    q0 = gaussian_noise(*n, seed=4)
+    a, _ = _run(sp, conv, 1, q0, 0.01, 1e-4, 23)
+    b, _ = _run(sp, conv, 5, q0, 0.01, 1e-4, 23, in_place=True)
+    assert np.array_equal(a, b)
+    p = orc.params(n, dx=1.0 / n[0], nu0=0.02, nufreq=60.0, cx=1.0, cy=-0.5, cz=0.25)
+    assert rel_l2(b, orc.rk4(p, q0, 0.01, 1e-4, 23)) < TOL64
+
+
 def test_autotuner_considers_cluster_path_and_unsupported_grids_are_refused(sp):
     conv = sp.Convection(32, 32, 32, 1.0 / 32, 0.01, 0.0, 1.0, 1.0, 1.0)
     t = conv.autotune(sp.SP_F64, 1)
@@ -101,12 +114,13 @@ def test_autotuner_considers_cluster_path_and_unsupported_grids_are_refused(sp):
 
 
 @pytest.mark.parametrize("kind", [3, 5])
-@pytest.mark.parametrize("skip,P", [(True, 6), (False, 6), (True, 40)])
+@pytest.mark.parametrize("skip,P", [(True, 6), (False, 6), (True, 16), (True, 40)])
 def test_parareal_fine_sweep_on_clusters_equals_stage_kernels(sp, skip, P, kind):
     """All slices' fine runs of a Parareal iteration in one launch, one cluster per
     slice (converged slices gated off on the device).  With 40 slices the z-slab
     clusters of 2 planes per CTA (8 CTAs each) would exceed the SMs, so the batch
-    runs clusters of 4 planes per CTA; the (y,z) blocks take fewer, larger blocks."""
+    runs clusters of 4 planes per CTA; the (y,z) blocks take 4 x 4 blocks for 6
+    and 40 slices and 2 x 4 blocks for 16."""
     n = 16
     outs = []
     for k in (1, kind):
